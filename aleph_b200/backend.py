@@ -1,0 +1,251 @@
+"""Host-side mirror of aleph's ``Backend`` trait over the engine's C ABI.
+
+``B200SvBackend`` has the trait's methods (crates/aleph-backend/src/lib.rs:86-163):
+``allocate``, ``apply_gate``, ``measure``, ``sample``, ``expectation_value``,
+``probabilities``, ``apply_diagonal_phase``, ``apply_tiled_block`` and
+``unpermute_state``; ``run`` / ``run_with_outcomes`` mirror the drivers of
+crates/aleph-backend/src/lib.rs:182-245. Errors raise :class:`BackendError`
+subclasses named after the reference's variants. Every call goes to the
+CUDA library; there is no host compute path.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import abi
+from .circuit import Circuit, DiagonalPhase, Flat, GateInstance, Measure, TiledBlock, flatten
+
+
+class BackendError(Exception):
+    """``BackendError`` (crates/aleph-backend/src/lib.rs:22-74)."""
+
+    variant = "BackendError"
+
+    def __init__(self, status: int, message: str, info: abi.ErrorInfo | None = None):
+        self.status = status
+        self.info = info
+        super().__init__(message)
+
+
+_ERRORS: dict[int, type] = {}
+for _code, _name in abi.STATUS_NAMES.items():
+    if _code == abi.OK:
+        continue
+    _ERRORS[_code] = type(_name, (BackendError,), {"variant": _name})
+    globals()[_name] = _ERRORS[_code]
+
+
+def _err(lib, handle, status):
+    buf = ct.create_string_buffer(512)
+    lib.aleph_b200_last_error(handle, buf, 512)
+    info = abi.ErrorInfo()
+    lib.aleph_b200_last_error_info(handle, ct.byref(info))
+    cls = _ERRORS.get(status, BackendError)
+    return cls(status, buf.value.decode(errors="replace") or abi.STATUS_NAMES.get(status, str(status)), info)
+
+
+@dataclass
+class State:
+    """A device-resident state vector owned by the caller (``CudaSvState``)."""
+
+    ptr: ct.c_void_p
+    num_qubits: int
+    backend: "B200SvBackend"
+
+    def free(self):
+        if self.ptr:
+            self.backend.lib.aleph_b200_free_state(self.backend.handle, self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+    def amplitudes(self) -> np.ndarray:
+        return self.backend.statevector(self)
+
+
+@dataclass
+class MeasurementRecord:
+    """``MeasurementRecord`` (crates/aleph-backend/src/lib.rs:188-195)."""
+
+    instruction_index: int
+    qubit: int
+    clbit: int
+    outcome: bool
+
+
+class B200SvBackend:
+    """The B200 dense state-vector backend (``--backend b200``).
+
+    precision: ``"f64"`` (complex128), ``"f32"`` (complex64, CUDA cores) or
+    ``"tc32"`` (complex64 with 6-qubit dense blocks on tcgen05 tensor cores).
+    """
+
+    def __init__(self, seed: int = 0, device: int = 0, precision: str = "f64"):
+        self.lib = abi.load_library()
+        h = ct.c_void_p()
+        st = self.lib.aleph_b200_create(int(seed) & (2**64 - 1), device, abi.PRECISION[precision], ct.byref(h))
+        if st != abi.OK:
+            raise BackendError(st, f"aleph_b200_create failed with status {abi.STATUS_NAMES.get(st, st)}")
+        self.handle = h
+        self.precision = precision
+
+    @classmethod
+    def with_seed(cls, seed: int, **kw) -> "B200SvBackend":
+        return cls(seed=seed, **kw)
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.aleph_b200_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, status):
+        if status != abi.OK:
+            raise _err(self.lib, self.handle, status)
+
+    def set_tuning(self, key: str, value: int) -> "B200SvBackend":
+        self._check(self.lib.aleph_b200_set_tuning(self.handle, key.encode(), int(value)))
+        return self
+
+    def set_qubit_cap(self, cap: int) -> "B200SvBackend":
+        self._check(self.lib.aleph_b200_set_qubit_cap(self.handle, cap))
+        return self
+
+    # ---- Backend trait -------------------------------------------------------
+    def allocate(self, num_qubits: int) -> State:
+        p = ct.c_void_p()
+        self._check(self.lib.aleph_b200_allocate(self.handle, num_qubits, ct.byref(p)))
+        return State(p, num_qubits, self)
+
+    def apply_gate(self, state: State, gate: GateInstance) -> None:
+        flat = flatten([gate])
+        self._check(self.lib.aleph_b200_apply_gate(self.handle, state.ptr, flat.instrs, flat.matrix_ptr,
+                                                   flat.matrix.size // 2))
+
+    def apply_diagonal_phase(self, state: State, dp: DiagonalPhase) -> None:
+        flat = flatten([dp])
+        self._check(self.lib.aleph_b200_apply_diagonal_phase(
+            self.handle, state.ptr, flat.terms if flat.n_terms else None, flat.n_terms,
+            flat.conds.ctypes.data_as(ct.POINTER(ct.c_uint64)) if flat.conds.size else None, flat.conds.size))
+
+    def apply_tiled_block(self, state: State, block: TiledBlock) -> None:
+        self.apply_stream(state, [block])
+
+    def unpermute_state(self, state: State, perm) -> None:
+        arr = (ct.c_uint32 * len(perm))(*perm)
+        self._check(self.lib.aleph_b200_unpermute(self.handle, state.ptr, arr, len(perm)))
+
+    def measure(self, state: State, qubit: int, u: float | None = None) -> bool:
+        o, c = ct.c_int(), ct.c_int()
+        self._check(self.lib.aleph_b200_measure(self.handle, state.ptr, qubit, -1.0 if u is None else float(u),
+                                                ct.byref(o), ct.byref(c)))
+        return bool(o.value)
+
+    def sample(self, state: State, shots: int, variates=None, mode: str = "auto") -> np.ndarray:
+        out = np.zeros(max(1, shots), dtype=np.uint64)
+        optr = out.ctypes.data_as(ct.POINTER(ct.c_uint64))
+        if variates is None:
+            self._check(self.lib.aleph_b200_sample_seeded(self.handle, state.ptr, shots, optr))
+            return out[:shots]
+        m = {"alias": abi.SAMPLE_ALIAS, "cumulative": abi.SAMPLE_CUMULATIVE, "auto": abi.SAMPLE_AUTO}[mode]
+        if m == abi.SAMPLE_AUTO:
+            m = abi.SAMPLE_ALIAS if shots >= 2 else abi.SAMPLE_CUMULATIVE
+        v = np.ascontiguousarray(np.asarray(variates, dtype=np.uint64 if m == abi.SAMPLE_ALIAS else np.float64))
+        if v.size < shots:
+            raise ValueError("need one variate per shot")
+        self._check(self.lib.aleph_b200_sample(self.handle, state.ptr, shots, m, v.ctypes.data_as(ct.c_void_p), optr))
+        return out[:shots]
+
+    def expectation_value(self, state: State, terms, coefficient: float = 1.0) -> float:
+        """``terms``: sequence of (qubit, 'I'|'X'|'Y'|'Z') — a ``PauliString``."""
+        k = len(terms)
+        qs = (ct.c_uint32 * max(1, k))(*[int(q) for q, _ in terms])
+        ps = (ct.c_uint8 * max(1, k))(*[abi.PAULI[p] for _, p in terms])
+        out = ct.c_double()
+        self._check(self.lib.aleph_b200_expectation(self.handle, state.ptr, qs, ps, k, float(coefficient),
+                                                    ct.byref(out)))
+        return out.value
+
+    def probabilities(self, state: State, qubits) -> np.ndarray:
+        k = len(qubits)
+        qs = (ct.c_uint32 * max(1, k))(*qubits)
+        out = np.zeros(1 << k, dtype=np.float64)
+        self._check(self.lib.aleph_b200_probabilities(self.handle, state.ptr, qs, k,
+                                                      out.ctypes.data_as(ct.POINTER(ct.c_double))))
+        return out
+
+    # ---- extras ----------------------------------------------------------------
+    def statevector(self, state: State) -> np.ndarray:
+        out = np.zeros(2 << state.num_qubits, dtype=np.float64)
+        self._check(self.lib.aleph_b200_get_amplitudes(self.handle, state.ptr,
+                                                       out.ctypes.data_as(ct.POINTER(ct.c_double))))
+        return out[0::2] + 1j * out[1::2]
+
+    def set_statevector(self, state: State, psi) -> None:
+        psi = np.asarray(psi, dtype=np.complex128)
+        buf = np.empty(2 * psi.size, dtype=np.float64)
+        buf[0::2] = psi.real
+        buf[1::2] = psi.imag
+        self._check(self.lib.aleph_b200_set_amplitudes(self.handle, state.ptr,
+                                                       buf.ctypes.data_as(ct.POINTER(ct.c_double))))
+
+    def norm_sqr(self, state: State) -> float:
+        out = ct.c_double()
+        self._check(self.lib.aleph_b200_norm_sqr(self.handle, state.ptr, ct.byref(out)))
+        return out.value
+
+    def synchronize(self):
+        self._check(self.lib.aleph_b200_synchronize(self.handle))
+
+    def stats(self) -> dict:
+        s = abi.Stats()
+        self.lib.aleph_b200_get_stats(self.handle, ct.byref(s))
+        return {k: getattr(s, k) for k, _ in abi.Stats._fields_}
+
+    def reset_stats(self):
+        self.lib.aleph_b200_reset_stats(self.handle)
+
+    def apply_stream(self, state: State, instructions, measure_uniforms=None, flat: Flat | None = None):
+        """Apply a whole instruction list in one call; returns measurement outcomes."""
+        flat = flat or flatten(instructions)
+        u = None if measure_uniforms is None else np.ascontiguousarray(np.asarray(measure_uniforms, np.float64))
+        outs = (ct.c_uint8 * max(1, flat.n))()
+        nout = ct.c_uint64()
+        self._check(self.lib.aleph_b200_apply_gate_stream(
+            self.handle, state.ptr, flat.instrs, flat.n, ct.byref(flat.pools),
+            u.ctypes.data_as(ct.POINTER(ct.c_double)) if u is not None and u.size else None,
+            0 if u is None else u.size, outs, flat.n, ct.byref(nout)))
+        return [int(outs[i]) for i in range(nout.value)]
+
+
+def run_with_outcomes(backend: B200SvBackend, circuit: Circuit, measure_uniforms=None):
+    """``run_with_outcomes`` (crates/aleph-backend/src/lib.rs:211-245)."""
+    if circuit.num_qubits == 0 and len(circuit) == 0:
+        raise EmptyCircuit(abi.EMPTY_CIRCUIT, "cannot run an empty circuit")  # noqa: F821
+    state = backend.allocate(circuit.num_qubits)
+    outs = backend.apply_stream(state, circuit.instructions, measure_uniforms)
+    records = []
+    k = 0
+    for idx, inst in enumerate(circuit.instructions):
+        if isinstance(inst, Measure):
+            records.append(MeasurementRecord(idx, inst.qubit, inst.clbit, bool(outs[k])))
+            k += 1
+    return state, records
+
+
+def run(backend: B200SvBackend, circuit: Circuit, measure_uniforms=None) -> State:
+    """``run`` (crates/aleph-backend/src/lib.rs:182-185)."""
+    state, _ = run_with_outcomes(backend, circuit, measure_uniforms)
+    return state

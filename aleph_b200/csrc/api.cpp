@@ -1,0 +1,822 @@
+// api.cpp — the C ABI of the B200 state-vector engine (include/aleph_b200.h).
+//
+// Host orchestration only: validation and lowering (planner.cpp), one
+// upload of the plan tables per call, stream-ordered kernel launches, and a
+// single synchronisation where a value must come back to the caller. There
+// is no host compute path: every amplitude update and every reduction runs
+// in the CUDA kernels of this library.
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "engine.h"
+
+using namespace ab;
+
+struct aleph_b200_handle : Handle {};
+struct aleph_b200_state : State {};
+
+namespace {
+
+// ---- per-handle RNG: xoshiro256** seeded through splitmix64 -----------------
+// It supplies the variates of aleph_b200_measure (u < 0) and
+// aleph_b200_sample_seeded. Explicit variates can always be passed instead,
+// which is how outcome parity with the reference is established.
+uint64_t splitmix64(uint64_t& x) {
+  uint64_t z = (x += 0x9e3779b97f4a7c15ull);
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+  return z ^ (z >> 31);
+}
+inline uint64_t rotl(uint64_t x, int k) { return (x << k) | (x >> (64 - k)); }
+
+struct HandleExt {
+  uint64_t rng[4];
+};
+HandleExt* ext(aleph_b200_handle* h);
+
+uint64_t rng_next(aleph_b200_handle* h) {
+  uint64_t* s = ext(h)->rng;
+  const uint64_t result = rotl(s[1] * 5, 7) * 9;
+  const uint64_t t = s[1] << 17;
+  s[2] ^= s[0];
+  s[3] ^= s[1];
+  s[1] ^= s[2];
+  s[0] ^= s[3];
+  s[2] ^= t;
+  s[3] = rotl(s[3], 45);
+  return result;
+}
+double rng_f64(aleph_b200_handle* h) { return (double)(rng_next(h) >> 11) * (1.0 / 9007199254740992.0); }
+
+struct FullHandle : aleph_b200_handle {
+  HandleExt x;
+};
+HandleExt* ext(aleph_b200_handle* h) { return &static_cast<FullHandle*>(h)->x; }
+
+// ---- errors -----------------------------------------------------------------
+int set_error(aleph_b200_handle* h, int status, const char* fmt, ...) {
+  if (!h) return status;
+  h->err.status = status;
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  std::vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  h->err_msg = buf;
+  return status;
+}
+
+// Display strings of BackendError (crates/aleph-backend/src/lib.rs:22-74).
+int report(aleph_b200_handle* h, const aleph_b200_error_info& e) {
+  h->err = e;
+  switch (e.status) {
+    case ALEPH_B200_OK: h->err_msg.clear(); return 0;
+    case ALEPH_B200_QUBIT_OUT_OF_RANGE:
+      return set_error(h, e.status, "qubit %u out of range for %u-qubit state", e.qubit, e.num_qubits);
+    case ALEPH_B200_DUPLICATE_QUBIT: return set_error(h, e.status, "duplicate qubit %u in gate or query", e.qubit);
+    case ALEPH_B200_ARITY_MISMATCH:
+      return set_error(h, e.status, "gate `%s` expects %u qubits, got %u", e.kind, e.expected, e.got);
+    case ALEPH_B200_UNSUPPORTED_GATE: return set_error(h, e.status, "gate `%s` is not supported by this backend", e.kind);
+    case ALEPH_B200_UNSUPPORTED_INSTRUCTION:
+      return set_error(h, e.status, "IR instruction `%s` is not supported by this backend", e.kind);
+    case ALEPH_B200_NON_FINITE_PARAM:
+      return set_error(h, e.status, "gate `%s` has a non-finite (NaN or infinite) parameter", e.kind);
+    case ALEPH_B200_NON_UNITARY_MATRIX:
+      return set_error(h, e.status, "user-supplied matrix is not unitary (max deviation = %e)", e.value);
+    case ALEPH_B200_DEGENERATE_MEASUREMENT:
+      return set_error(h, e.status, "measurement of qubit %u on degenerate branch (p = %e)", e.qubit, e.value);
+    case ALEPH_B200_TOO_MANY_QUBITS:
+      return set_error(h, e.status, "requested %u qubits exceeds backend limit of %u", e.requested, e.limit);
+    case ALEPH_B200_INVALID_PAULI_STRING:
+      return set_error(h, e.status, "Pauli string violates its invariants: %s", e.kind);
+    case ALEPH_B200_INVALID_STATE: return set_error(h, e.status, "backend state is invalid: %s", e.kind);
+    case ALEPH_B200_EMPTY_CIRCUIT: return set_error(h, e.status, "cannot run an empty circuit");
+    default: return set_error(h, e.status, "%s", e.kind[0] ? e.kind : "invalid argument");
+  }
+}
+
+int cuda_fail(aleph_b200_handle* h, cudaError_t err, const char* what) {
+  h->err = aleph_b200_error_info{};
+  h->err.status = ALEPH_B200_DEVICE_FAILURE;
+  return set_error(h, ALEPH_B200_DEVICE_FAILURE, "device operation failed: %s: %s", what, cudaGetErrorString(err));
+}
+
+#define CK(expr, what)                                   \
+  do {                                                   \
+    cudaError_t _e = (expr);                             \
+    if (_e != cudaSuccess) return cuda_fail(h, _e, what); \
+  } while (0)
+
+int ensure(aleph_b200_handle* h, Scratch& s, size_t bytes) {
+  if (s.bytes >= bytes) return 0;
+  if (s.ptr) {
+    cudaStreamSynchronize(h->stream);
+    cudaFree(s.ptr);
+    s.ptr = nullptr;
+    s.bytes = 0;
+  }
+  size_t want = bytes < 4096 ? 4096 : bytes;
+  cudaError_t e = cudaMalloc(&s.ptr, want);
+  if (e != cudaSuccess) {
+    s.ptr = nullptr;
+    return cuda_fail(h, e, "scratch allocation");
+  }
+  s.bytes = want;
+  return 0;
+}
+
+int bind(aleph_b200_handle* h) {
+  cudaError_t e = cudaSetDevice(h->device);
+  if (e != cudaSuccess) return cuda_fail(h, e, "cudaSetDevice");
+  return 0;
+}
+
+// ---- plan upload + execution --------------------------------------------------
+struct DevPlan {
+  Op* ops;
+  void* coef;
+  PolyTables poly;
+  double* uniforms;
+  int32_t* status;
+  uint8_t* outcomes;
+};
+
+size_t al(size_t x) { return (x + 255) & ~(size_t)255; }
+
+int execute(aleph_b200_handle* h, aleph_b200_state* st, const Plan& P, const double* uniforms, uint32_t n_uniforms,
+            std::vector<int32_t>* status_out, std::vector<uint8_t>* outcomes_out) {
+  const bool f64 = st->precision == ALEPH_B200_F64;
+  // host image of the device tables
+  std::vector<float> coef32;
+  if (!f64) {
+    coef32.resize(P.coef.size());
+    for (size_t i = 0; i < P.coef.size(); ++i) coef32[i] = (float)P.coef[i];
+  }
+  const size_t b_ops = al(P.ops.size() * sizeof(Op));
+  const size_t b_coef = al(f64 ? P.coef.size() * 8 : coef32.size() * 4);
+  const size_t b_pa = al(P.poly_angle.size() * 8), b_po = al(P.poly_off.size() * 4), b_pc = al(P.poly_cnt.size() * 4),
+               b_pd = al(P.poly_conds.size() * 8);
+  const size_t b_u = al((size_t)n_uniforms * 8), b_s = al(64), b_o = al(P.n_measures + 1);
+  const size_t total = b_ops + b_coef + b_pa + b_po + b_pc + b_pd + b_u + b_s + b_o;
+  if (int r = ensure(h, h->plan_buf, total)) return r;
+  std::vector<uint8_t> img(total, 0);
+  size_t off = 0;
+  auto put = [&](const void* src, size_t bytes, size_t span) -> size_t {
+    const size_t at = off;
+    if (bytes) std::memcpy(img.data() + off, src, bytes);
+    off += span;
+    return at;
+  };
+  const size_t o_ops = put(P.ops.data(), P.ops.size() * sizeof(Op), b_ops);
+  const size_t o_coef = f64 ? put(P.coef.data(), P.coef.size() * 8, b_coef) : put(coef32.data(), coef32.size() * 4, b_coef);
+  const size_t o_pa = put(P.poly_angle.data(), P.poly_angle.size() * 8, b_pa);
+  const size_t o_po = put(P.poly_off.data(), P.poly_off.size() * 4, b_po);
+  const size_t o_pc = put(P.poly_cnt.data(), P.poly_cnt.size() * 4, b_pc);
+  const size_t o_pd = put(P.poly_conds.data(), P.poly_conds.size() * 8, b_pd);
+  const size_t o_u = put(uniforms, (size_t)n_uniforms * 8, b_u);
+  const size_t o_s = put(nullptr, 0, b_s);
+  const size_t o_o = put(nullptr, 0, b_o);
+  CK(cudaMemcpyAsync(h->plan_buf.ptr, img.data(), total, cudaMemcpyHostToDevice, h->stream), "plan upload");
+  char* base = (char*)h->plan_buf.ptr;
+  DevPlan d;
+  d.ops = (Op*)(base + o_ops);
+  d.coef = base + o_coef;
+  d.poly.angle = (const double*)(base + o_pa);
+  d.poly.cond_off = (const uint32_t*)(base + o_po);
+  d.poly.cond_cnt = (const uint32_t*)(base + o_pc);
+  d.poly.conds = (const uint64_t*)(base + o_pd);
+  d.uniforms = (double*)(base + o_u);
+  d.status = (int32_t*)(base + o_s);
+  d.outcomes = (uint8_t*)(base + o_o);
+
+  const uint32_t nb = reduce_blocks(st->n, h->sm_count);
+  if (P.n_measures) {
+    if (int r = ensure(h, h->reduce, (size_t)nb * 3 * 8 + 256)) return r;
+  }
+  const double bpa = f64 ? 16.0 : 8.0;
+  const double len = (double)(1ull << st->n);
+  uint32_t mi = 0;
+  for (const Pass& ps : P.passes) {
+    cudaError_t e = cudaSuccess;
+    switch (ps.kind) {
+      case PASS_TILE:
+        e = launch_tile_pass(st->amps, st->precision, ps.tile, d.ops, d.coef, d.poly, h->stream);
+        h->stats.tile_passes++;
+        h->stats.passes++;
+        h->stats.algorithmic_bytes += 2 * len * bpa;
+        break;
+      case PASS_SMEM:
+        e = launch_smem_pass(st->amps, st->precision, st->n, d.ops + ps.tile.op_begin, ps.tile.op_count, d.coef, d.poly,
+                             h->stream);
+        h->stats.passes++;
+        h->stats.algorithmic_bytes += 2 * len * bpa;
+        break;
+      case PASS_KQ:
+        e = launch_kq_pass(st->amps, st->precision, st->n, d.ops + ps.tile.op_begin, P.ops[ps.tile.op_begin], d.coef,
+                           h->stream);
+        h->stats.passes++;
+        h->stats.algorithmic_bytes += 2 * len * bpa;
+        break;
+      case PASS_MEASURE:
+        e = launch_measure_pass(st->amps, st->precision, st->n, ps.qubit, (double*)h->reduce.ptr, nb, d.uniforms,
+                                n_uniforms, d.status, d.outcomes + mi, h->stream);
+        ++mi;
+        h->stats.kernel_launches += 3;
+        h->stats.algorithmic_bytes += 3 * len * bpa;
+        break;
+      case PASS_BLOCK:
+        e = cudaErrorNotSupported;
+        break;
+    }
+    if (e != cudaSuccess) return cuda_fail(h, e, "kernel launch");
+    h->stats.kernel_launches++;
+    h->stats.gates_planned += ps.gates;
+  }
+  if (status_out || outcomes_out || P.n_measures) {
+    std::vector<int32_t> stv(16, 0);
+    CK(cudaMemcpyAsync(stv.data(), d.status, 16 * 4, cudaMemcpyDeviceToHost, h->stream), "status readback");
+    std::vector<uint8_t> oc(P.n_measures + 1, 0);
+    if (P.n_measures)
+      CK(cudaMemcpyAsync(oc.data(), d.outcomes, P.n_measures, cudaMemcpyDeviceToHost, h->stream), "outcome readback");
+    CK(cudaStreamSynchronize(h->stream), "stream synchronize");
+    if (status_out) *status_out = stv;
+    if (outcomes_out) {
+      oc.resize(P.n_measures);
+      *outcomes_out = oc;
+    }
+    if (stv[0] != 0 && !status_out) {
+      aleph_b200_error_info e{};
+      e.status = stv[0];
+      e.qubit = (uint32_t)stv[2];
+      return report(h, e);
+    }
+  }
+  return 0;
+}
+
+bool valid_handle(aleph_b200_handle* h) { return h != nullptr; }
+
+}  // namespace
+
+extern "C" {
+
+int aleph_b200_create(uint64_t seed, int device, int precision, aleph_b200_handle** out) {
+  if (!out) return ALEPH_B200_INVALID_ARGUMENT;
+  *out = nullptr;
+  if (precision < ALEPH_B200_F64 || precision > ALEPH_B200_TC32) return ALEPH_B200_INVALID_ARGUMENT;
+  FullHandle* h = new (std::nothrow) FullHandle();
+  if (!h) return ALEPH_B200_DEVICE_FAILURE;
+  h->device = device;
+  h->precision = precision;
+  h->qubit_cap = precision == ALEPH_B200_F64 ? 33 : 34;
+  h->opts.tile_r = precision == ALEPH_B200_F64 ? 4 : 4;
+  uint64_t x = seed;
+  for (int i = 0; i < 4; ++i) h->x.rng[i] = splitmix64(x);
+  cudaError_t e = cudaSetDevice(device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, device);
+  if (e != cudaSuccess) {
+    delete h;
+    return ALEPH_B200_DEVICE_FAILURE;
+  }
+  *out = h;
+  return ALEPH_B200_OK;
+}
+
+int aleph_b200_destroy(aleph_b200_handle* h) {
+  if (!h) return ALEPH_B200_OK;
+  cudaSetDevice(h->device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  for (Scratch* s : {&h->reduce, &h->plan_buf, &h->sample, &h->status})
+    if (s->ptr) cudaFree(s->ptr);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete static_cast<FullHandle*>(h);
+  return ALEPH_B200_OK;
+}
+
+int aleph_b200_set_qubit_cap(aleph_b200_handle* h, uint32_t cap) {
+  if (!h) return ALEPH_B200_INVALID_ARGUMENT;
+  h->qubit_cap = cap;
+  return ALEPH_B200_OK;
+}
+
+int aleph_b200_allocate(aleph_b200_handle* h, uint32_t n, aleph_b200_state** out) {
+  if (!h || !out) return ALEPH_B200_INVALID_ARGUMENT;
+  *out = nullptr;
+  if (n > h->qubit_cap || n > 40) {
+    aleph_b200_error_info e{};
+    e.status = ALEPH_B200_TOO_MANY_QUBITS;
+    e.requested = n;
+    e.limit = h->qubit_cap;
+    return report(h, e);
+  }
+  if (int r = bind(h)) return r;
+  aleph_b200_state* st = new (std::nothrow) aleph_b200_state();
+  if (!st) return set_error(h, ALEPH_B200_DEVICE_FAILURE, "host allocation failed");
+  st->n = n;
+  st->precision = h->precision == ALEPH_B200_F64 ? ALEPH_B200_F64 : ALEPH_B200_F32;
+  st->bytes = (size_t)(st->precision == ALEPH_B200_F64 ? 16 : 8) << n;
+  cudaError_t e = cudaMalloc(&st->amps, st->bytes);
+  if (e != cudaSuccess) {
+    delete st;
+    cudaGetLastError();
+    return cuda_fail(h, e, "state allocation");
+  }
+  e = launch_init_zero_state(st->amps, n, st->precision, h->stream);
+  if (e != cudaSuccess) {
+    cudaFree(st->amps);
+    delete st;
+    return cuda_fail(h, e, "state init");
+  }
+  h->stats.kernel_launches++;
+  *out = st;
+  return ALEPH_B200_OK;
+}
+
+int aleph_b200_free_state(aleph_b200_handle* h, aleph_b200_state* st) {
+  if (!st) return ALEPH_B200_OK;
+  if (h) {
+    cudaSetDevice(h->device);
+    cudaStreamSynchronize(h->stream);
+  }
+  cudaFree(st->amps);
+  delete st;
+  return ALEPH_B200_OK;
+}
+
+int aleph_b200_num_qubits(const aleph_b200_state* st, uint32_t* out) {
+  if (!st || !out) return ALEPH_B200_INVALID_ARGUMENT;
+  *out = st->n;
+  return ALEPH_B200_OK;
+}
+
+int aleph_b200_apply_gate(aleph_b200_handle* h, aleph_b200_state* st, const aleph_b200_instr* g, const double* pool,
+                          uint64_t pool_len) {
+  if (!h || !st || !g) return ALEPH_B200_INVALID_ARGUMENT;
+  if (g->kind >= 28) {
+    aleph_b200_error_info e{};
+    e.status = ALEPH_B200_UNSUPPORTED_GATE;
+    std::snprintf(e.kind, sizeof(e.kind), "%s", gate_name(g->kind));
+    return report(h, e);
+  }
+  if (int r = bind(h)) return r;
+  std::vector<Lowered> ops(1);
+  aleph_b200_error_info e{};
+  if (int s = lower_gate(*g, st->n, pool, pool_len, &ops[0], &e)) return report(h, e);
+  Plan P;
+  build_plan(ops, st->n, h->opts, &P);
+  return execute(h, st, P, nullptr, 0, nullptr, nullptr);
+}
+
+static int stream_impl(aleph_b200_handle* h, aleph_b200_state* st, const aleph_b200_instr* in, uint64_t count,
+                       const aleph_b200_pools* pools, const double* mu, uint64_t n_mu, uint8_t* outcomes,
+                       uint64_t outcomes_cap, uint64_t* n_outcomes, int32_t* used_out) {
+  if (!h || !st || (!in && count)) return ALEPH_B200_INVALID_ARGUMENT;
+  if (int r = bind(h)) return r;
+  if (n_outcomes) *n_outcomes = 0;
+  const double* pool = pools ? pools->matrix_pool : nullptr;
+  const uint64_t pool_len = pools ? pools->matrix_pool_len : 0;
+  std::vector<Lowered> ops;
+  ops.reserve(count);
+  for (uint64_t i = 0; i < count; ++i) {
+    const aleph_b200_instr& g = in[i];
+    aleph_b200_error_info e{};
+    e.instruction = (uint32_t)i;
+    if (g.kind < 28) {
+      ops.emplace_back();
+      if (lower_gate(g, st->n, pool, pool_len, &ops.back(), &e)) return report(h, e);
+      ops.back().record = (uint32_t)i;
+    } else if (g.kind == ALEPH_INSTR_MEASURE) {
+      if (g.num_qubits != 1) {
+        e.status = ALEPH_B200_INVALID_ARGUMENT;
+        std::snprintf(e.kind, sizeof(e.kind), "measure record");
+        return report(h, e);
+      }
+      if (g.qubits[0] >= st->n) {
+        e.status = ALEPH_B200_QUBIT_OUT_OF_RANGE;
+        e.qubit = g.qubits[0];
+        e.num_qubits = st->n;
+        return report(h, e);
+      }
+      ops.emplace_back();
+      std::memset(&ops.back().op, 0, sizeof(Op));
+      ops.back().is_measure = true;
+      ops.back().measure_qubit = g.qubits[0];
+      ops.back().record = (uint32_t)i;
+    } else if (g.kind == ALEPH_INSTR_RESET) {
+      e.status = ALEPH_B200_UNSUPPORTED_INSTRUCTION;
+      std::snprintf(e.kind, sizeof(e.kind), "reset");
+      return report(h, e);
+    } else if (g.kind == ALEPH_INSTR_BARRIER || g.kind == ALEPH_INSTR_TILED_BLOCK) {
+      continue;  // barrier: no-op; tiled block: its gates follow as plain records
+    } else if (g.kind == ALEPH_INSTR_DIAGONAL_PHASE) {
+      if (!pools || g.data_offset + g.data_len > pools->n_terms || (g.data_len && !pools->terms)) {
+        e.status = ALEPH_B200_INVALID_ARGUMENT;
+        std::snprintf(e.kind, sizeof(e.kind), "diagonal phase terms");
+        return report(h, e);
+      }
+      ops.emplace_back();
+      if (lower_diagonal_phase(pools->terms + g.data_offset, g.data_len, pools->cond_pool, pools->n_conds, &ops.back(),
+                               &e))
+        return report(h, e);
+      ops.back().record = (uint32_t)i;
+    } else {
+      e.status = ALEPH_B200_UNSUPPORTED_INSTRUCTION;
+      std::snprintf(e.kind, sizeof(e.kind), "%s", gate_name(g.kind));
+      return report(h, e);
+    }
+  }
+  Plan P;
+  build_plan(ops, st->n, h->opts, &P);
+  // measurement variates: explicit, or drawn from the handle RNG (only the consumed ones advance it)
+  std::vector<double> drawn;
+  uint64_t saved[4];
+  std::memcpy(saved, ext(h)->rng, sizeof(saved));
+  if (!mu && P.n_measures) {
+    drawn.resize(P.n_measures);
+    for (auto& u : drawn) u = rng_f64(h);
+    mu = drawn.data();
+    n_mu = drawn.size();
+  }
+  std::vector<int32_t> stv;
+  std::vector<uint8_t> oc;
+  if (int r = execute(h, st, P, mu, (uint32_t)n_mu, &stv, &oc)) return r;
+  if (!drawn.empty()) {
+    std::memcpy(ext(h)->rng, saved, sizeof(saved));
+    for (int32_t k = 0; k < stv[1]; ++k) rng_next(h);
+  }
+  if (stv[0] != 0) {
+    aleph_b200_error_info e{};
+    e.status = stv[0];
+    e.qubit = (uint32_t)stv[2];
+    if (e.status == ALEPH_B200_INVALID_STATE)
+      std::snprintf(e.kind, sizeof(e.kind), "state norm deviates from 1 beyond drift budget");
+    else if (e.status == ALEPH_B200_INVALID_ARGUMENT)
+      std::snprintf(e.kind, sizeof(e.kind), "measure uniforms exhausted");
+    return report(h, e);
+  }
+  if (outcomes)
+    for (size_t i = 0; i < oc.size() && i < outcomes_cap; ++i) outcomes[i] = oc[i];
+  if (n_outcomes) *n_outcomes = oc.size();
+  if (used_out) *used_out = stv.empty() ? 0 : stv[1];
+  return ALEPH_B200_OK;
+}
+
+int aleph_b200_apply_gate_stream(aleph_b200_handle* h, aleph_b200_state* st, const aleph_b200_instr* in, uint64_t count,
+                                 const aleph_b200_pools* pools, const double* mu, uint64_t n_mu, uint8_t* outcomes,
+                                 uint64_t outcomes_cap, uint64_t* n_outcomes) {
+  return stream_impl(h, st, in, count, pools, mu, n_mu, outcomes, outcomes_cap, n_outcomes, nullptr);
+}
+
+int aleph_b200_apply_diagonal_phase(aleph_b200_handle* h, aleph_b200_state* st, const aleph_b200_phase_term* terms,
+                                    uint64_t n_terms, const uint64_t* conds, uint64_t n_conds) {
+  if (!h || !st || (!terms && n_terms)) return ALEPH_B200_INVALID_ARGUMENT;
+  if (int r = bind(h)) return r;
+  std::vector<Lowered> ops(1);
+  aleph_b200_error_info e{};
+  if (lower_diagonal_phase(terms, n_terms, conds, n_conds, &ops[0], &e)) return report(h, e);
+  Plan P;
+  build_plan(ops, st->n, h->opts, &P);
+  return execute(h, st, P, nullptr, 0, nullptr, nullptr);
+}
+
+int aleph_b200_unpermute(aleph_b200_handle* h, aleph_b200_state* st, const uint32_t* perm, uint32_t n) {
+  if (!h || !st || !perm) return ALEPH_B200_INVALID_ARGUMENT;
+  if (n != st->n) return set_error(h, ALEPH_B200_INVALID_ARGUMENT, "perm length %u != num_qubits %u", n, st->n);
+  uint64_t seen = 0;
+  for (uint32_t i = 0; i < n; ++i) {
+    if (perm[i] >= n || ((seen >> perm[i]) & 1))
+      return set_error(h, ALEPH_B200_INVALID_ARGUMENT, "perm is not a permutation of 0..%u", n);
+    seen |= 1ull << perm[i];
+  }
+  if (int r = bind(h)) return r;
+  void* tmp = nullptr;
+  CK(cudaMalloc(&tmp, st->bytes), "unpermute buffer");
+  uint32_t* dperm = nullptr;
+  cudaError_t e = cudaMalloc(&dperm, 64 * 4);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dperm, perm, n * 4, cudaMemcpyHostToDevice, h->stream);
+  if (e == cudaSuccess) e = launch_unpermute(st->amps, tmp, st->precision, n, dperm, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) {
+    cudaFree(tmp);
+    cudaFree(dperm);
+    return cuda_fail(h, e, "unpermute");
+  }
+  cudaFree(st->amps);
+  cudaFree(dperm);
+  st->amps = tmp;
+  h->stats.kernel_launches++;
+  return ALEPH_B200_OK;
+}
+
+int aleph_b200_measure(aleph_b200_handle* h, aleph_b200_state* st, uint32_t qubit, double u, int* outcome,
+                       int* consumed) {
+  if (!h || !st || !outcome) return ALEPH_B200_INVALID_ARGUMENT;
+  if (qubit >= st->n) {
+    aleph_b200_error_info e{};
+    e.status = ALEPH_B200_QUBIT_OUT_OF_RANGE;
+    e.qubit = qubit;
+    e.num_qubits = st->n;
+    return report(h, e);
+  }
+  aleph_b200_instr rec{};
+  rec.kind = ALEPH_INSTR_MEASURE;
+  rec.num_qubits = 1;
+  rec.qubits[0] = qubit;
+  uint8_t oc = 0;
+  uint64_t nout = 0;
+  int32_t used = 0;
+  const int r = u < 0.0 ? stream_impl(h, st, &rec, 1, nullptr, nullptr, 0, &oc, 1, &nout, &used)
+                        : stream_impl(h, st, &rec, 1, nullptr, &u, 1, &oc, 1, &nout, &used);
+  if (r) return r;
+  *outcome = oc;
+  if (consumed) *consumed = used;
+  return ALEPH_B200_OK;
+}
+
+static int check_norm_host(aleph_b200_handle* h, aleph_b200_state* st, double* norm_out) {
+  const uint32_t nb = reduce_blocks(st->n, h->sm_count);
+  if (int r = ensure(h, h->reduce, (size_t)nb * 3 * 8 + 256)) return r;
+  double* part = (double*)h->reduce.ptr;
+  double* out2 = part + 3 * (size_t)nb;
+  CK(launch_norm(st->amps, st->precision, st->n, part, nb, out2, h->stream), "norm");
+  h->stats.kernel_launches += 2;
+  double res[2];
+  CK(cudaMemcpyAsync(res, out2, 16, cudaMemcpyDeviceToHost, h->stream), "norm readback");
+  CK(cudaStreamSynchronize(h->stream), "stream synchronize");
+  if (norm_out) *norm_out = res[0];
+  const double len = (double)(1ull << st->n);
+  if (res[1] > 0.0) {
+    aleph_b200_error_info e{};
+    e.status = ALEPH_B200_INVALID_STATE;
+    std::snprintf(e.kind, sizeof(e.kind), "non-finite amplitude norm2");
+    return report(h, e);
+  }
+  if (!std::isfinite(res[0]) || std::fabs(res[0] - 1.0) > std::sqrt(len) * 1e-10) {
+    aleph_b200_error_info e{};
+    e.status = ALEPH_B200_INVALID_STATE;
+    std::snprintf(e.kind, sizeof(e.kind), "state norm2 deviates from 1");
+    return report(h, e);
+  }
+  return 0;
+}
+
+int aleph_b200_sample(aleph_b200_handle* h, aleph_b200_state* st, uint32_t shots, int mode, const void* variates,
+                      uint64_t* out) {
+  if (!h || !st || (shots && (!variates || !out))) return ALEPH_B200_INVALID_ARGUMENT;
+  if (mode == ALEPH_B200_SAMPLE_AUTO) mode = shots >= 2 ? ALEPH_B200_SAMPLE_ALIAS : ALEPH_B200_SAMPLE_CUMULATIVE;
+  if (mode != ALEPH_B200_SAMPLE_ALIAS && mode != ALEPH_B200_SAMPLE_CUMULATIVE)
+    return set_error(h, ALEPH_B200_INVALID_ARGUMENT, "unknown sample mode %d", mode);
+  if (mode == ALEPH_B200_SAMPLE_ALIAS && st->n > 28)
+    return set_error(h, ALEPH_B200_INVALID_ARGUMENT, "alias sampling supports n <= 28; use CUMULATIVE");
+  if (int r = bind(h)) return r;
+  if (shots == 0) return check_norm_host(h, st, nullptr);
+  const size_t sb = sample_scratch_bytes(st->n, mode, shots);
+  const size_t vb = (size_t)shots * 8;
+  if (int r = ensure(h, h->sample, al(sb) + 2 * al(vb) + 256)) return r;
+  char* base = (char*)h->sample.ptr;
+  void* dvar = base + al(sb);
+  uint64_t* dout = (uint64_t*)(base + al(sb) + al(vb));
+  int32_t* dstatus = (int32_t*)(base + al(sb) + 2 * al(vb));
+  CK(cudaMemsetAsync(dstatus, 0, 64, h->stream), "status clear");
+  CK(cudaMemsetAsync(base, 0, sb, h->stream), "scratch clear");
+  CK(cudaMemcpyAsync(dvar, variates, vb, cudaMemcpyHostToDevice, h->stream), "variates upload");
+  CK(launch_sample(st->amps, st->precision, st->n, shots, mode, dvar, dout, base, sb, dstatus, h->sm_count, h->stream),
+     "sample");
+  h->stats.kernel_launches += mode == ALEPH_B200_SAMPLE_ALIAS ? 7 : 5;
+  int32_t status[4];
+  CK(cudaMemcpyAsync(status, dstatus, 16, cudaMemcpyDeviceToHost, h->stream), "status readback");
+  CK(cudaMemcpyAsync(out, dout, vb, cudaMemcpyDeviceToHost, h->stream), "sample readback");
+  CK(cudaStreamSynchronize(h->stream), "stream synchronize");
+  if (status[0]) {
+    aleph_b200_error_info e{};
+    e.status = status[0];
+    std::snprintf(e.kind, sizeof(e.kind), "state norm2 deviates from 1");
+    return report(h, e);
+  }
+  return ALEPH_B200_OK;
+}
+
+int aleph_b200_sample_seeded(aleph_b200_handle* h, aleph_b200_state* st, uint32_t shots, uint64_t* out) {
+  if (!h || !st || (shots && !out)) return ALEPH_B200_INVALID_ARGUMENT;
+  if (shots >= 2) {
+    std::vector<uint64_t> w(shots);
+    for (auto& x : w) x = rng_next(h);
+    return aleph_b200_sample(h, st, shots, ALEPH_B200_SAMPLE_ALIAS, w.data(), out);
+  }
+  double u = shots ? rng_f64(h) : 0.0;
+  return aleph_b200_sample(h, st, shots, ALEPH_B200_SAMPLE_CUMULATIVE, &u, out);
+}
+
+int aleph_b200_expectation(aleph_b200_handle* h, aleph_b200_state* st, const uint32_t* qubits, const uint8_t* paulis,
+                           uint32_t nt, double coefficient, double* out) {
+  if (!h || !st || !out || (nt && (!qubits || !paulis))) return ALEPH_B200_INVALID_ARGUMENT;
+  if (int r = bind(h)) return r;
+  const uint32_t nb = reduce_blocks(st->n, h->sm_count);
+  if (int r = ensure(h, h->reduce, (size_t)nb * 3 * 8 + 256)) return r;
+  uint64_t xm = 0, zm = 0;
+  uint32_t ny = 0;
+  bool bad_pauli = false;
+  for (uint32_t t = 0; t < nt; ++t) {
+    if (qubits[t] >= 64) continue;
+    switch (paulis[t]) {
+      case ALEPH_PAULI_I: break;
+      case ALEPH_PAULI_X: xm |= 1ull << qubits[t]; break;
+      case ALEPH_PAULI_Y: xm |= 1ull << qubits[t]; zm |= 1ull << qubits[t]; ++ny; break;
+      case ALEPH_PAULI_Z: zm |= 1ull << qubits[t]; break;
+      default: bad_pauli = true;
+    }
+  }
+  double* part = (double*)h->reduce.ptr;
+  double* out3 = part + 3 * (size_t)nb;
+  const bool valid_q = [&] {
+    for (uint32_t t = 0; t < nt; ++t)
+      if (qubits[t] >= st->n) return false;
+    return true;
+  }();
+  CK(launch_expectation(st->amps, st->precision, st->n, valid_q ? xm : 0, valid_q ? zm : 0, ny, part, nb, out3,
+                        h->stream),
+     "expectation");
+  h->stats.kernel_launches += 2;
+  double res[3];
+  CK(cudaMemcpyAsync(res, out3, 24, cudaMemcpyDeviceToHost, h->stream), "expectation readback");
+  CK(cudaStreamSynchronize(h->stream), "stream synchronize");
+  // validate_state first (measure.rs:166), then coefficient, then qubits (measure.rs:172-193)
+  const double len = (double)(1ull << st->n);
+  if (res[1] > 0.0 || !std::isfinite(res[0]) || std::fabs(res[0] - 1.0) > std::sqrt(len) * 1e-10) {
+    aleph_b200_error_info e{};
+    e.status = ALEPH_B200_INVALID_STATE;
+    std::snprintf(e.kind, sizeof(e.kind), "state norm2 deviates from 1");
+    return report(h, e);
+  }
+  if (!std::isfinite(coefficient)) {
+    aleph_b200_error_info e{};
+    e.status = ALEPH_B200_INVALID_PAULI_STRING;
+    std::snprintf(e.kind, sizeof(e.kind), "non-finite coefficient");
+    return report(h, e);
+  }
+  for (uint32_t t = 0; t < nt; ++t) {
+    aleph_b200_error_info e{};
+    if (qubits[t] >= st->n) {
+      e.status = ALEPH_B200_QUBIT_OUT_OF_RANGE;
+      e.qubit = qubits[t];
+      e.num_qubits = st->n;
+      return report(h, e);
+    }
+    for (uint32_t j = 0; j < t; ++j)
+      if (qubits[j] == qubits[t]) {
+        e.status = ALEPH_B200_DUPLICATE_QUBIT;
+        e.qubit = qubits[t];
+        return report(h, e);
+      }
+  }
+  if (bad_pauli) return set_error(h, ALEPH_B200_INVALID_ARGUMENT, "unknown Pauli code");
+  *out = coefficient * res[2];
+  return ALEPH_B200_OK;
+}
+
+int aleph_b200_probabilities(aleph_b200_handle* h, aleph_b200_state* st, const uint32_t* qubits, uint32_t k,
+                             double* out) {
+  if (!h || !st || !out || (k && !qubits)) return ALEPH_B200_INVALID_ARGUMENT;
+  if (int r = bind(h)) return r;
+  // validate_state first (measure.rs:245)
+  if (int r = check_norm_host(h, st, nullptr)) return r;
+  for (uint32_t t = 0; t < k; ++t) {
+    aleph_b200_error_info e{};
+    if (qubits[t] >= st->n) {
+      e.status = ALEPH_B200_QUBIT_OUT_OF_RANGE;
+      e.qubit = qubits[t];
+      e.num_qubits = st->n;
+      return report(h, e);
+    }
+    for (uint32_t j = 0; j < t; ++j)
+      if (qubits[j] == qubits[t]) {
+        e.status = ALEPH_B200_DUPLICATE_QUBIT;
+        e.qubit = qubits[t];
+        return report(h, e);
+      }
+  }
+  if (k == 0) {
+    out[0] = 1.0;
+    return ALEPH_B200_OK;
+  }
+  const uint32_t nb = reduce_blocks(st->n, h->sm_count);
+  const size_t dim = (size_t)1 << k;
+  const size_t part_bytes = k <= 10 ? (size_t)nb * (dim + 2) * 8 : (size_t)nb * 3 * 8;
+  if (int r = ensure(h, h->reduce, part_bytes + 256)) return r;
+  if (int r = ensure(h, h->sample, dim * 8 + 256)) return r;
+  uint32_t* dq = nullptr;
+  CK(cudaMalloc(&dq, 64 * 4), "qubit list");
+  cudaError_t e = cudaMemcpyAsync(dq, qubits, k * 4, cudaMemcpyHostToDevice, h->stream);
+  double* dout = (double*)h->sample.ptr;
+  double* dnorm = dout + dim;
+  if (e == cudaSuccess)
+    e = launch_probabilities(st->amps, st->precision, st->n, dq, k, (double*)h->reduce.ptr, nb, dout, dnorm, h->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(out, dout, dim * 8, cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  cudaFree(dq);
+  if (e != cudaSuccess) return cuda_fail(h, e, "probabilities");
+  h->stats.kernel_launches += 2;
+  return ALEPH_B200_OK;
+}
+
+int aleph_b200_get_amplitudes(aleph_b200_handle* h, aleph_b200_state* st, double* out) {
+  if (!h || !st || !out) return ALEPH_B200_INVALID_ARGUMENT;
+  if (int r = bind(h)) return r;
+  const uint64_t len = 1ull << st->n;
+  if (st->precision == ALEPH_B200_F64) {
+    CK(cudaMemcpyAsync(out, st->amps, st->bytes, cudaMemcpyDeviceToHost, h->stream), "amplitude readback");
+    CK(cudaStreamSynchronize(h->stream), "stream synchronize");
+    return ALEPH_B200_OK;
+  }
+  std::vector<float> tmp(2 * len);
+  CK(cudaMemcpyAsync(tmp.data(), st->amps, st->bytes, cudaMemcpyDeviceToHost, h->stream), "amplitude readback");
+  CK(cudaStreamSynchronize(h->stream), "stream synchronize");
+  for (uint64_t i = 0; i < 2 * len; ++i) out[i] = tmp[i];
+  return ALEPH_B200_OK;
+}
+
+int aleph_b200_set_amplitudes(aleph_b200_handle* h, aleph_b200_state* st, const double* in) {
+  if (!h || !st || !in) return ALEPH_B200_INVALID_ARGUMENT;
+  if (int r = bind(h)) return r;
+  const uint64_t len = 1ull << st->n;
+  if (st->precision == ALEPH_B200_F64) {
+    CK(cudaMemcpyAsync(st->amps, in, st->bytes, cudaMemcpyHostToDevice, h->stream), "amplitude upload");
+    CK(cudaStreamSynchronize(h->stream), "stream synchronize");
+    return ALEPH_B200_OK;
+  }
+  std::vector<float> tmp(2 * len);
+  for (uint64_t i = 0; i < 2 * len; ++i) tmp[i] = (float)in[i];
+  CK(cudaMemcpyAsync(st->amps, tmp.data(), st->bytes, cudaMemcpyHostToDevice, h->stream), "amplitude upload");
+  CK(cudaStreamSynchronize(h->stream), "stream synchronize");
+  return ALEPH_B200_OK;
+}
+
+int aleph_b200_norm_sqr(aleph_b200_handle* h, aleph_b200_state* st, double* out) {
+  if (!h || !st || !out) return ALEPH_B200_INVALID_ARGUMENT;
+  if (int r = bind(h)) return r;
+  const uint32_t nb = reduce_blocks(st->n, h->sm_count);
+  if (int r = ensure(h, h->reduce, (size_t)nb * 3 * 8 + 256)) return r;
+  double* part = (double*)h->reduce.ptr;
+  double* out2 = part + 3 * (size_t)nb;
+  CK(launch_norm(st->amps, st->precision, st->n, part, nb, out2, h->stream), "norm");
+  h->stats.kernel_launches += 2;
+  double res[2];
+  CK(cudaMemcpyAsync(res, out2, 16, cudaMemcpyDeviceToHost, h->stream), "norm readback");
+  CK(cudaStreamSynchronize(h->stream), "stream synchronize");
+  *out = res[1] > 0.0 ? NAN : res[0];
+  return ALEPH_B200_OK;
+}
+
+int aleph_b200_synchronize(aleph_b200_handle* h) {
+  if (!h) return ALEPH_B200_INVALID_ARGUMENT;
+  if (int r = bind(h)) return r;
+  CK(cudaStreamSynchronize(h->stream), "stream synchronize");
+  return ALEPH_B200_OK;
+}
+
+int aleph_b200_last_error(const aleph_b200_handle* h, char* buf, uint64_t len) {
+  if (!h || !buf || !len) return ALEPH_B200_INVALID_ARGUMENT;
+  std::snprintf(buf, len, "%s", h->err_msg.c_str());
+  return h->err.status;
+}
+
+int aleph_b200_last_error_info(const aleph_b200_handle* h, aleph_b200_error_info* out) {
+  if (!h || !out) return ALEPH_B200_INVALID_ARGUMENT;
+  *out = h->err;
+  return h->err.status;
+}
+
+int aleph_b200_set_tuning(aleph_b200_handle* h, const char* key, int64_t value) {
+  if (!h || !key) return ALEPH_B200_INVALID_ARGUMENT;
+  if (!std::strcmp(key, "tile_r")) {
+    if (value < 1 || value > 5) return set_error(h, ALEPH_B200_INVALID_ARGUMENT, "tile_r must be in 1..5");
+    h->opts.tile_r = (uint32_t)value;
+    return ALEPH_B200_OK;
+  }
+  if (!std::strcmp(key, "smem_max_n")) {
+    if (value < 0 || value > 12) return set_error(h, ALEPH_B200_INVALID_ARGUMENT, "smem_max_n must be in 0..12");
+    h->opts.smem_max_n = (uint32_t)value;
+    return ALEPH_B200_OK;
+  }
+  return set_error(h, ALEPH_B200_INVALID_ARGUMENT, "unknown tuning key %s", key);
+}
+
+int aleph_b200_get_stats(const aleph_b200_handle* h, aleph_b200_stats* out) {
+  if (!h || !out) return ALEPH_B200_INVALID_ARGUMENT;
+  *out = h->stats;
+  return ALEPH_B200_OK;
+}
+
+int aleph_b200_reset_stats(aleph_b200_handle* h) {
+  if (!h) return ALEPH_B200_INVALID_ARGUMENT;
+  h->stats = aleph_b200_stats{};
+  return ALEPH_B200_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,195 @@
+// engine.h — internal declarations shared by the host planner/ABI (C++) and
+// the CUDA kernels of the B200 state-vector engine.
+#pragma once
+
+#include <cstdint>
+#include <cstddef>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/aleph_b200.h"
+
+namespace ab {
+
+// ---------------------------------------------------------------------------
+// Device ops. A gate is lowered to one Op; passes apply ordered Op lists.
+// ---------------------------------------------------------------------------
+enum OpType : uint8_t {
+  OP_1Q = 1,      // dense 2x2 on one target (coef: 4 complex, row-major)
+  OP_2Q = 2,      // dense 4x4 on two targets, q[0] = matrix MSB (coef: 16 complex)
+  OP_X = 3,       // Pauli-X permutation on one target (no arithmetic)
+  OP_CPHASE = 4,  // amp *= coef[0] where every bit of `mask` is 1 (Z, S, T, Phase, CZ, CCZ, ...)
+  OP_DIAG = 5,    // amp *= coef[idx], idx = bits of q[0..nq) MSB-first (nq <= 3)
+  OP_POLY = 6,    // DiagonalPhase: amp *= exp(i*phi(x)), terms [mask, mask+aux)
+  OP_KQ = 7,      // dense 2^k x 2^k, k = nq (3..5), q MSB-first (coef: 4^k complex)
+  OP_NEG = 8,     // amp = -amp where every bit of `mask` is 1 (CZ, CCZ, Z fast path)
+};
+
+struct Op {
+  uint8_t type;
+  uint8_t nq;      // target count in q[]
+  uint8_t a, b;    // tile slots of q[0] / q[1] (tile kernel); see TilePass
+  uint8_t q[6];    // global target qubits, MSB-first
+  uint8_t pad[2];
+  uint64_t ctrl;   // global control mask: op acts where (x & ctrl) == ctrl
+  uint64_t mask;   // OP_CPHASE / OP_NEG: qubit mask; OP_POLY: first term index
+  uint32_t coef;   // offset into the coefficient pool (complex elements)
+  uint32_t aux;    // OP_POLY: term count
+};
+static_assert(sizeof(Op) == 40, "Op layout");
+
+// Diagonal-phase polynomial tables (OP_POLY), device-resident per plan.
+struct PolyTables {
+  const double* angle;
+  const uint32_t* cond_off;
+  const uint32_t* cond_cnt;
+  const uint64_t* conds;
+};
+
+// Warp-tile pass: lanes hold qubits 0..4 (one amplitude per lane), each
+// thread holds 2^R amplitudes over the R "register" qubits hq[0..R).
+// Slot numbering of Op::a/b: 0..4 = lane bit (= qubit), 5+j = register bit j.
+struct TilePass {
+  uint32_t n;
+  uint32_t R;
+  uint32_t hq[5];
+  uint32_t op_begin;
+  uint32_t op_count;
+  uint32_t pad;
+};
+
+// Tensor-core dense-block pass (TC32): a 2^6 x 2^6 complex matrix on the
+// qubits bq[0..6) (ascending; bq[j] = bit j of the block row index), with
+// diagonal ops applied before (pre) and after (post) the block product.
+struct BlockPass {
+  uint32_t n;
+  uint32_t bq[6];
+  uint32_t mat;        // offset of the split BF16 operand images in the block pool (bytes)
+  uint32_t pre_begin, pre_count, post_begin, post_count;
+};
+
+enum PassKind : uint8_t { PASS_TILE = 1, PASS_SMEM = 2, PASS_KQ = 3, PASS_MEASURE = 4, PASS_BLOCK = 5 };
+
+struct Pass {
+  PassKind kind;
+  TilePass tile;       // PASS_TILE (also op range for PASS_SMEM / PASS_KQ)
+  BlockPass block;     // PASS_BLOCK
+  uint32_t qubit;      // PASS_MEASURE
+  uint32_t record;     // instruction index (errors, outcome slot)
+  uint32_t gates;      // gates consumed (stats / cost model)
+};
+
+// ---------------------------------------------------------------------------
+// Host-side lowered gate (validated) and plans.
+// ---------------------------------------------------------------------------
+struct Lowered {
+  Op op;
+  std::vector<double> coef;  // complex pairs (re, im)
+  uint64_t nondiag;          // qubits the op acts on non-diagonally
+  uint64_t diag;             // qubits the op reads only diagonally (controls, diagonal targets)
+  uint32_t record;           // source instruction index
+  bool is_measure = false;
+  uint32_t measure_qubit = 0;
+  // OP_POLY terms (DiagonalPhase): angle, condition count, condition masks
+  std::vector<double> poly_angle;
+  std::vector<uint32_t> poly_cnt;
+  std::vector<uint64_t> poly_conds;
+};
+
+struct Plan {
+  std::vector<Pass> passes;
+  std::vector<Op> ops;
+  std::vector<double> coef;  // complex pairs
+  // OP_POLY tables
+  std::vector<double> poly_angle;
+  std::vector<uint32_t> poly_off, poly_cnt;
+  std::vector<uint64_t> poly_conds;
+  // TC32 split-BF16 block operand images (bytes), one 64 KiB image per block
+  std::vector<uint8_t> block_images;
+  uint32_t n_measures = 0;
+};
+
+struct PlanOptions {
+  uint32_t tile_r = 5;          // register qubits per warp tile
+  uint32_t smem_max_n = 12;     // states with n <= this run as one shared-memory pass
+  bool tensor_blocks = false;   // TC32: fuse into 6-qubit dense blocks
+  uint32_t block_k = 6;
+};
+
+// ---------------------------------------------------------------------------
+// Engine objects.
+// ---------------------------------------------------------------------------
+struct State {
+  uint32_t n = 0;
+  int precision = ALEPH_B200_F64;
+  void* amps = nullptr;   // double2[2^n] or float2[2^n]
+  size_t bytes = 0;
+};
+
+struct Scratch {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+};
+
+struct Handle {
+  int device = 0;
+  int precision = ALEPH_B200_F64;
+  uint32_t qubit_cap = 33;
+  cudaStream_t stream = nullptr;
+  uint64_t rng_state[2] = {0, 0};
+  aleph_b200_error_info err{};
+  std::string err_msg;
+  aleph_b200_stats stats{};
+  PlanOptions opts;
+  int sm_count = 148;
+  // device scratch (grown on demand, freed with the handle)
+  Scratch reduce;    // reduction partials
+  Scratch plan_buf;  // uploaded plan tables
+  Scratch sample;    // sampling tables
+  Scratch status;    // device status words (measure outcomes, error flags)
+};
+
+// kernels_*.cu entry points (host wrappers; all launch on `stream`)
+cudaError_t launch_init_zero_state(void* amps, uint32_t n, int precision, cudaStream_t s);
+cudaError_t launch_tile_pass(void* amps, int precision, const TilePass& p, const Op* ops, const void* coef,
+                             PolyTables poly, cudaStream_t s);
+cudaError_t launch_smem_pass(void* amps, int precision, uint32_t n, const Op* ops, uint32_t op_count,
+                             const void* coef, PolyTables poly, cudaStream_t s);
+cudaError_t launch_kq_pass(void* amps, int precision, uint32_t n, const Op* op_dev, const Op& op_host,
+                           const void* coef, cudaStream_t s);
+cudaError_t launch_block_pass(void* amps, const BlockPass& p, const uint8_t* images, const Op* ops,
+                              const void* coef, PolyTables poly, int* dev_error, int sm_count, cudaStream_t s);
+cudaError_t launch_convert(const void* src, int src_prec, void* dst, int dst_prec, uint64_t count, cudaStream_t s);
+cudaError_t launch_unpermute(const void* src, void* dst, int precision, uint32_t n, const uint32_t* perm_dev,
+                             cudaStream_t s);
+
+// readout (kernels_readout.cu)
+// partial sums: out[0] = sum |a|^2, out[1] = count of non-finite |a|^2
+cudaError_t launch_norm(const void* amps, int precision, uint32_t n, double* partials, uint32_t nblocks,
+                        double* out2, cudaStream_t s);
+cudaError_t launch_measure_pass(void* amps, int precision, uint32_t n, uint32_t qubit, double* partials,
+                                uint32_t nblocks, const double* uniforms, uint32_t n_uniforms, int32_t* status,
+                                uint8_t* outcome_slot, cudaStream_t s);
+cudaError_t launch_expectation(const void* amps, int precision, uint32_t n, uint64_t xmask, uint64_t zmask,
+                               uint32_t ny, double* partials, uint32_t nblocks, double* out3, cudaStream_t s);
+cudaError_t launch_probabilities(const void* amps, int precision, uint32_t n, const uint32_t* qubits_dev, uint32_t k,
+                                 double* partials, uint32_t nblocks, double* out, double* norm_out, cudaStream_t s);
+uint32_t reduce_blocks(uint32_t n, int sm_count);
+
+// sampling (kernels_sample.cu)
+size_t sample_scratch_bytes(uint32_t n, int mode, uint32_t shots);
+cudaError_t launch_sample(const void* amps, int precision, uint32_t n, uint32_t shots, int mode, const void* variates_dev,
+                          uint64_t* out_dev, void* scratch, size_t scratch_bytes, int32_t* status, int sm_count,
+                          cudaStream_t s);
+
+// planner (planner.cpp)
+int lower_gate(const aleph_b200_instr& g, uint32_t n, const double* pool, uint64_t pool_len, Lowered* out,
+               aleph_b200_error_info* err);
+int lower_diagonal_phase(const aleph_b200_phase_term* terms, uint64_t n_terms, const uint64_t* conds, uint64_t n_conds,
+                         Lowered* out, aleph_b200_error_info* err);
+const char* gate_name(uint32_t kind);
+int build_plan(const std::vector<Lowered>& ops, uint32_t n, const PlanOptions& o, Plan* plan);
+
+}  // namespace ab

@@ -1,0 +1,407 @@
+// kernels_sample.cu — on-device shot sampling with the reference's exact
+// seed-to-outcome mappings, given the same variates.
+//
+// ALIAS (the reference's shots >= 2 path, crates/aleph-sv/src/measure.rs:109-124):
+//   probabilities p_i = re*re + im*im rounded exactly like the CPU (no FMA),
+//   Vose's table built by AliasTable::build (crates/aleph-sv/src/sampling.rs:104-167)
+//   with the same LIFO stack discipline and the same floating-point operation
+//   order, so the table is bit-identical; the table build's sequential chain
+//   runs on one thread (it is inherently sequential), the O(N) partition and
+//   all draws run in parallel. Draw: index = (word >> 32) & (N-1),
+//   u = (u32)word * 2^-32, u < prob[i] ? i : alias[i] (sampling.rs:179-197).
+// CUMULATIVE (the reference's shots <= 1 path, sampling.rs:59-91): the
+//   inverse CDF of the sequential left-to-right prefix sum with strict
+//   `target < cumulative`, zero bins skipped, last positive bin as fallback.
+//   Shots are resolved in parallel on a two-level prefix (tree block sums +
+//   a sequential scan inside the block); a shot whose target lies within the
+//   rounding bound of a bin boundary is re-resolved by an exact sequential
+//   scan (for n <= 26), so the outcome equals the sequential CPU result.
+
+#include <cmath>
+
+#include "common.cuh"
+
+namespace ab {
+
+constexpr uint32_t CUM_BLOCK = 2048;  // amplitudes per level-1 CDF block
+constexpr uint32_t EXACT_MAX_N = 26;  // exact re-resolution of ambiguous shots up to this n
+
+template <typename Real>
+__device__ __forceinline__ double prob_exact(const V2<Real>* amps, uint64_t i) {
+  const V2<Real> a = ld_amp<Real>(amps + i);
+  const double x = (double)a.x, y = (double)a.y;
+  return __dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y));
+}
+
+// ------------------------------------------------------------------ ALIAS ----
+struct AliasScratch {
+  double* prob;       // N: scaled probabilities, then the table thresholds
+  uint32_t* alias;    // N
+  uint32_t* small;    // N: indices with scaled < 1, ascending
+  uint32_t* large;    // N: indices with scaled >= 1, ascending
+  uint32_t* bcount;   // 2 * nb: per-block small / large counts, then exclusive offsets
+  uint32_t* totals;   // 2: small / large counts
+  double* normsum;    // 2 * nb partial [sum p, non-finite]
+};
+
+constexpr uint32_t PART_B = 1024;  // elements per partition block
+
+template <typename Real>
+__global__ void alias_scale_kernel(const V2<Real>* __restrict__ amps, uint64_t len, AliasScratch s) {
+  // one block per PART_B elements: scaled values + per-block small/large counts + norm partials
+  __shared__ uint32_t cs[32], cl[32];
+  __shared__ double ns[32], nb[32];
+  const double nf = (double)len;
+  const uint64_t i = (uint64_t)blockIdx.x * PART_B + threadIdx.x;
+  uint32_t small = 0, large = 0;
+  double psum = 0.0, bad = 0.0;
+  if (i < len) {
+    const double p = prob_exact<Real>(amps, i);
+    if (!isfinite(p)) bad = 1.0;
+    else psum = p;
+    const double sc = __dmul_rn(nf, p);
+    s.prob[i] = sc;
+    if (sc < 1.0) small = 1;
+    else large = 1;
+  }
+  const unsigned bs = __ballot_sync(0xffffffffu, small), bl = __ballot_sync(0xffffffffu, large);
+  for (int o = 16; o; o >>= 1) {
+    psum += __shfl_down_sync(0xffffffffu, psum, o);
+    bad += __shfl_down_sync(0xffffffffu, bad, o);
+  }
+  const int w = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0) {
+    cs[w] = __popc(bs);
+    cl[w] = __popc(bl);
+    ns[w] = psum;
+    nb[w] = bad;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t a = 0, b = 0;
+    double x = 0.0, y = 0.0;
+    for (int k = 0; k < (int)(PART_B / 32); ++k) {
+      a += cs[k];
+      b += cl[k];
+      x += ns[k];
+      y += nb[k];
+    }
+    s.bcount[2 * blockIdx.x] = a;
+    s.bcount[2 * blockIdx.x + 1] = b;
+    s.normsum[2 * blockIdx.x] = x;
+    s.normsum[2 * blockIdx.x + 1] = y;
+  }
+}
+
+// Exclusive scan of the per-block counts (one thread; nb <= 2^18 blocks).
+__global__ void alias_offsets_kernel(AliasScratch s, uint32_t nblocks, double* norm_out) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  uint32_t a = 0, b = 0;
+  double x = 0.0, y = 0.0;
+  for (uint32_t k = 0; k < nblocks; ++k) {
+    const uint32_t ca = s.bcount[2 * k], cb = s.bcount[2 * k + 1];
+    s.bcount[2 * k] = a;
+    s.bcount[2 * k + 1] = b;
+    a += ca;
+    b += cb;
+    x += s.normsum[2 * k];
+    y += s.normsum[2 * k + 1];
+  }
+  s.totals[0] = a;
+  s.totals[1] = b;
+  norm_out[0] = x;
+  norm_out[1] = y;
+}
+
+__global__ void alias_partition_kernel(uint64_t len, AliasScratch s) {
+  __shared__ uint32_t ws[32], wl[32];
+  const uint64_t i = (uint64_t)blockIdx.x * PART_B + threadIdx.x;
+  bool is_small = false, valid = i < len;
+  if (valid) is_small = s.prob[i] < 1.0;
+  const unsigned bs = __ballot_sync(0xffffffffu, valid && is_small);
+  const unsigned bl = __ballot_sync(0xffffffffu, valid && !is_small);
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) {
+    ws[w] = __popc(bs);
+    wl[w] = __popc(bl);
+  }
+  __syncthreads();
+  uint32_t os = s.bcount[2 * blockIdx.x], ol = s.bcount[2 * blockIdx.x + 1];
+  for (int k = 0; k < w; ++k) {
+    os += ws[k];
+    ol += wl[k];
+  }
+  const unsigned below = (1u << lane) - 1u;
+  if (valid) {
+    if (is_small) s.small[os + __popc(bs & below)] = (uint32_t)i;
+    else s.large[ol + __popc(bl & below)] = (uint32_t)i;
+  }
+}
+
+// The Vose loop of AliasTable::build with both stacks' tops tracked exactly.
+// status[0] is set on failure (never expected: the loop is bounded by N).
+__global__ void alias_chain_kernel(uint64_t len, AliasScratch s, int32_t* status) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  if (len == 1) {
+    s.prob[0] = 1.0;
+    s.alias[0] = 0;
+    return;
+  }
+  int64_t ts = (int64_t)s.totals[0];  // small stack height (stack = small[0..ts))
+  int64_t tl = (int64_t)s.totals[1];  // large stack height
+  uint32_t* SS = s.small;
+  uint32_t* LS = s.large;
+  uint64_t guard = 0;
+  while (ts > 0 && tl > 0) {
+    if (++guard > 2 * len + 4) {
+      status[0] = ALEPH_B200_DEVICE_FAILURE;
+      return;
+    }
+    const uint32_t sidx = SS[--ts];
+    const uint32_t lidx = LS[--tl];
+    const double ss = s.prob[sidx];
+    const double sl = s.prob[lidx];
+    s.prob[sidx] = ss;  // threshold = scaled[s]
+    s.alias[sidx] = lidx;
+    const double nl = __dsub_rn(__dadd_rn(sl, ss), 1.0);
+    s.prob[lidx] = nl;
+    if (nl < 1.0) SS[ts++] = lidx;
+    else LS[tl++] = lidx;
+  }
+  // leftovers: self-alias with threshold 1 (drained by a parallel kernel below)
+  s.totals[0] = (uint32_t)ts;
+  s.totals[1] = (uint32_t)tl;
+}
+
+__global__ void alias_drain_kernel(AliasScratch s) {
+  const uint32_t ts = s.totals[0], tl = s.totals[1];
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < ts + tl; k += gridDim.x * blockDim.x) {
+    const uint32_t i = k < ts ? s.small[k] : s.large[k - ts];
+    s.prob[i] = 1.0;
+    s.alias[i] = i;
+  }
+}
+
+__global__ void alias_draw_kernel(AliasScratch s, uint64_t mask, const uint64_t* __restrict__ words, uint32_t shots,
+                                  uint64_t* __restrict__ out) {
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < shots; k += gridDim.x * blockDim.x) {
+    const uint64_t bits = words[k];
+    const uint64_t i = (bits >> 32) & mask;
+    const double u = (double)(uint32_t)bits * (1.0 / 4294967296.0);
+    out[k] = u < s.prob[i] ? i : (uint64_t)s.alias[i];
+  }
+}
+
+// Norm check of validate_state (sampling.rs:36-57): sets status on failure.
+__global__ void check_norm_kernel(const double* norm2, uint64_t len, int32_t* status) {
+  if (threadIdx.x != 0) return;
+  const double total = norm2[0];
+  if (norm2[1] > 0.0 || !isfinite(total) || fabs(total - 1.0) > sqrt((double)len) * 1e-10)
+    status[0] = ALEPH_B200_INVALID_STATE;
+}
+
+// ------------------------------------------------------------- CUMULATIVE ----
+struct CumScratch {
+  double* bsum;      // nb + 1: block sums, then exclusive block prefix (bsum[nb] = total)
+  double* norm;      // 2: [total, non-finite count]
+  uint32_t* namb;    // ambiguous shot count
+  uint32_t* amb;     // shots: ambiguous shot ids
+};
+
+template <typename Real>
+__global__ void cum_blocks_kernel(const V2<Real>* __restrict__ amps, uint64_t len, CumScratch c) {
+  __shared__ double red[2][8];
+  const uint64_t b0 = (uint64_t)blockIdx.x * CUM_BLOCK;
+  double x = 0.0, bad = 0.0;
+  for (uint32_t j = threadIdx.x; j < CUM_BLOCK && b0 + j < len; j += blockDim.x) {
+    const double p = prob_exact<Real>(amps, b0 + j);
+    if (isfinite(p)) x += p;
+    else bad += 1.0;
+  }
+  for (int o = 16; o; o >>= 1) {
+    x += __shfl_down_sync(0xffffffffu, x, o);
+    bad += __shfl_down_sync(0xffffffffu, bad, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    red[0][threadIdx.x >> 5] = x;
+    red[1][threadIdx.x >> 5] = bad;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0, b = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+      s += red[0][w];
+      b += red[1][w];
+    }
+    c.bsum[blockIdx.x] = s;
+    if (b > 0.0) atomicAdd(&c.norm[1], b);
+  }
+}
+
+__global__ void cum_prefix_kernel(CumScratch c, uint32_t nb) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double run = 0.0;
+  for (uint32_t b = 0; b < nb; ++b) {
+    const double x = c.bsum[b];
+    c.bsum[b] = run;
+    run += x;
+  }
+  c.bsum[nb] = run;
+  c.norm[0] = run;
+}
+
+template <typename Real>
+__global__ void cum_draw_kernel(const V2<Real>* __restrict__ amps, uint64_t len, uint32_t nb, CumScratch c,
+                                const double* __restrict__ uniforms, uint32_t shots, uint64_t* __restrict__ out,
+                                int32_t* status) {
+  const double total = c.bsum[nb];
+  // Bound on |sequential - two-level| for prefixes and for u * total.
+  const double E = 8.0 * ((double)len + 64.0) * 1.1102230246251565e-16 * total;
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < shots; k += gridDim.x * blockDim.x) {
+    const double target = uniforms[k] * total;
+    // last block whose exclusive prefix <= target
+    uint32_t lo = 0, hi = nb;  // invariant: prefix[lo] <= target (prefix[0] = 0)
+    while (hi - lo > 1) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (c.bsum[mid] <= target) lo = mid;
+      else hi = mid;
+    }
+    double cum = c.bsum[lo];
+    double margin = fabs(target - cum);
+    int64_t found = -1, last_pos = -1;
+    for (uint64_t i = (uint64_t)lo * CUM_BLOCK; i < len; ++i) {
+      const double p = prob_exact<Real>(amps, i);
+      if (p > 0.0) {
+        last_pos = (int64_t)i;
+        cum += p;
+        margin = fmin(margin, fabs(cum - target));
+        if (target < cum) {
+          found = (int64_t)i;
+          break;
+        }
+      }
+    }
+    if (found < 0) {
+      // ran off the end: the last positive bin at or after the start block,
+      // or, if none, any earlier positive bin (resolved exactly below)
+      found = last_pos;
+      margin = 0.0;
+    }
+    out[k] = (uint64_t)(found < 0 ? 0 : found);
+    if (margin <= E) {
+      const uint32_t slot = atomicAdd(c.namb, 1u);
+      c.amb[slot] = k;
+    }
+  }
+}
+
+// Exact sequential resolution of the ambiguous shots: the reference's
+// validate_norm total and cumulative_index scan, element by element.
+template <typename Real>
+__global__ void cum_exact_kernel(const V2<Real>* __restrict__ amps, uint64_t len, CumScratch c,
+                                 const double* __restrict__ uniforms, uint64_t* __restrict__ out, int32_t* status) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const uint32_t na = *c.namb;
+  if (na == 0) return;
+  double total = 0.0;
+  for (uint64_t i = 0; i < len; ++i) total += prob_exact<Real>(amps, i);
+  // insertion-sort the ambiguous shots by target (they are few)
+  uint32_t* ids = c.amb;
+  for (uint32_t a = 1; a < na; ++a)
+    for (uint32_t b = a; b > 0 && uniforms[ids[b - 1]] > uniforms[ids[b]]; --b) {
+      const uint32_t t = ids[b];
+      ids[b] = ids[b - 1];
+      ids[b - 1] = t;
+    }
+  uint32_t next = 0;
+  double cum = 0.0;
+  int64_t last_pos = -1;
+  for (uint64_t i = 0; i < len && next < na; ++i) {
+    const double p = prob_exact<Real>(amps, i);
+    if (p > 0.0) {
+      last_pos = (int64_t)i;
+      cum += p;
+      while (next < na && uniforms[ids[next]] * total < cum) out[ids[next++]] = i;
+    }
+  }
+  if (last_pos < 0) {
+    status[0] = ALEPH_B200_INVALID_STATE;
+    return;
+  }
+  while (next < na) out[ids[next++]] = (uint64_t)last_pos;
+}
+
+size_t sample_scratch_bytes(uint32_t n, int mode, uint32_t shots) {
+  const uint64_t len = 1ull << n;
+  if (mode == ALEPH_B200_SAMPLE_ALIAS) {
+    const uint64_t nb = (len + PART_B - 1) / PART_B;
+    return len * (8 + 4 + 4 + 4) + nb * (8 + 16) + 256;
+  }
+  const uint64_t nb = (len + CUM_BLOCK - 1) / CUM_BLOCK;
+  return (nb + 1) * 8 + 64 + 256 + (size_t)shots * 4;
+}
+
+static inline char* align_up(char* p, size_t a) {
+  return (char*)(((uintptr_t)p + a - 1) & ~(uintptr_t)(a - 1));
+}
+
+cudaError_t launch_sample(const void* amps, int precision, uint32_t n, uint32_t shots, int mode, const void* variates,
+                          uint64_t* out, void* scratch, size_t scratch_bytes, int32_t* status, int sm_count,
+                          cudaStream_t st) {
+  const uint64_t len = 1ull << n;
+  const bool f64 = precision == ALEPH_B200_F64;
+  char* p = (char*)scratch;
+  if (mode == ALEPH_B200_SAMPLE_ALIAS) {
+    const uint32_t nb = (uint32_t)((len + PART_B - 1) / PART_B);
+    AliasScratch s;
+    s.prob = (double*)p; p += len * 8;
+    s.normsum = (double*)p; p += (size_t)nb * 16;
+    s.alias = (uint32_t*)p; p += len * 4;
+    s.small = (uint32_t*)p; p += len * 4;
+    s.large = (uint32_t*)p; p += len * 4;
+    s.bcount = (uint32_t*)p; p += (size_t)nb * 8;
+    p = align_up(p, 16);
+    s.totals = (uint32_t*)p; p += 16;
+    double* norm2 = (double*)p; p += 16;
+    if ((size_t)(p - (char*)scratch) > scratch_bytes) return cudaErrorInvalidValue;
+    if (f64) alias_scale_kernel<double><<<nb, PART_B, 0, st>>>((const double2*)amps, len, s);
+    else alias_scale_kernel<float><<<nb, PART_B, 0, st>>>((const float2*)amps, len, s);
+    alias_offsets_kernel<<<1, 32, 0, st>>>(s, nb, norm2);
+    check_norm_kernel<<<1, 32, 0, st>>>(norm2, len, status);
+    alias_partition_kernel<<<nb, PART_B, 0, st>>>(len, s);
+    alias_chain_kernel<<<1, 32, 0, st>>>(len, s, status);
+    alias_drain_kernel<<<(unsigned)sm_count * 4, 256, 0, st>>>(s);
+    if (shots)
+      alias_draw_kernel<<<(shots + 255) / 256, 256, 0, st>>>(s, len - 1, (const uint64_t*)variates, shots, out);
+    return cudaGetLastError();
+  }
+  const uint32_t nb = (uint32_t)((len + CUM_BLOCK - 1) / CUM_BLOCK);
+  CumScratch c;
+  c.bsum = (double*)p; p += ((size_t)nb + 1) * 8;
+  p = align_up(p, 16);
+  c.norm = (double*)p; p += 16;
+  c.namb = (uint32_t*)p; p += 16;
+  c.amb = (uint32_t*)align_up(p, 16);
+  p = (char*)(c.amb + shots);
+  if ((size_t)(p - (char*)scratch) > scratch_bytes) return cudaErrorInvalidValue;
+  cudaMemsetAsync(c.norm, 0, 32, st);
+  if (f64) cum_blocks_kernel<double><<<nb, 256, 0, st>>>((const double2*)amps, len, c);
+  else cum_blocks_kernel<float><<<nb, 256, 0, st>>>((const float2*)amps, len, c);
+  cum_prefix_kernel<<<1, 32, 0, st>>>(c, nb);
+  check_norm_kernel<<<1, 32, 0, st>>>(c.norm, len, status);
+  if (shots) {
+    if (f64)
+      cum_draw_kernel<double><<<(shots + 127) / 128, 128, 0, st>>>((const double2*)amps, len, nb, c,
+                                                                   (const double*)variates, shots, out, status);
+    else
+      cum_draw_kernel<float><<<(shots + 127) / 128, 128, 0, st>>>((const float2*)amps, len, nb, c,
+                                                                  (const double*)variates, shots, out, status);
+    if (n <= EXACT_MAX_N) {
+      if (f64) cum_exact_kernel<double><<<1, 32, 0, st>>>((const double2*)amps, len, c, (const double*)variates, out, status);
+      else cum_exact_kernel<float><<<1, 32, 0, st>>>((const float2*)amps, len, c, (const double*)variates, out, status);
+    }
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace ab

@@ -1,0 +1,606 @@
+// planner.cpp — gate validation, lowering to device ops, and pass planning.
+//
+// Validation follows NaiveSvBackend::apply_gate (crates/aleph-sv/src/backend.rs:74-152)
+// in the same order, with the same error variants: arity, then range and
+// duplicates over qubits followed by controls, UnitaryKq validation
+// (crates/aleph-sv/src/validation.rs:113-155), matrix materialisation
+// (Gate::matrix, crates/aleph-core/src/gate/kinds.rs:213-400) and the
+// unitarity check (validation.rs:25-51, AMPLITUDE_TOL = 1e-10).
+//
+// Planning: the gate list is cut into HBM passes. A warp-tile pass owns
+// qubits 0..4 plus R "register" qubits; the planner walks the pending gates
+// in order and takes every gate that (a) commutes past all gates it defers
+// and (b) acts non-diagonally only on tile qubits — diagonal gates (CZ,
+// phases, DiagonalPhase) and controls may sit on any qubit. This is the
+// greedy open-block idea of FuseKq (crates/aleph-ir/src/passes/fuse_kq.rs:144-400)
+// applied to cache tiles instead of matrices: no matrix is ever formed, the
+// gates run in registers one after the other.
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+
+#include "engine.h"
+
+namespace ab {
+
+namespace {
+
+struct Cx {
+  double re, im;
+};
+inline Cx mul(Cx a, Cx b) { return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re}; }
+inline Cx add(Cx a, Cx b) { return {a.re + b.re, a.im + b.im}; }
+inline Cx sub(Cx a, Cx b) { return {a.re - b.re, a.im - b.im}; }
+inline Cx conj(Cx a) { return {a.re, -a.im}; }
+inline Cx neg(Cx a) { return {-a.re, -a.im}; }
+
+constexpr double kTol = 1e-10;  // AMPLITUDE_TOL, crates/aleph-core/src/lib.rs:53
+
+void set_kind(aleph_b200_error_info* e, const char* k) { std::snprintf(e->kind, sizeof(e->kind), "%s", k); }
+int fail(aleph_b200_error_info* e, int s) {
+  e->status = s;
+  return s;
+}
+
+int arity(const aleph_b200_instr& g) {
+  switch (g.kind) {
+    case ALEPH_GATE_CNOT: case ALEPH_GATE_CZ: case ALEPH_GATE_SWAP: case ALEPH_GATE_ISWAP:
+    case ALEPH_GATE_ISWAPDG: case ALEPH_GATE_CRX: case ALEPH_GATE_CRY: case ALEPH_GATE_CRZ:
+    case ALEPH_GATE_UNITARY2Q: case ALEPH_GATE_UNITARY2QDIAG:
+      return 2;
+    case ALEPH_GATE_TOFFOLI: case ALEPH_GATE_CCZ:
+      return 3;
+    case ALEPH_GATE_UNITARYKQ:
+      return (int)g.aux;
+    default:
+      return g.kind < 28 ? 1 : -1;
+  }
+}
+
+// Gate::matrix (kinds.rs:213-400). Returns dim or 0 (error set).
+int matrix_of(const aleph_b200_instr& g, const double* pool, uint64_t pool_len, Cx m[8][8],
+              aleph_b200_error_info* e) {
+  const Cx z{0, 0}, o{1, 0};
+  for (int i = 0; i < 8; ++i)
+    for (int j = 0; j < 8; ++j) m[i][j] = z;
+  for (int i = 0; i < 3; ++i) {
+    const bool used = (g.kind >= ALEPH_GATE_RX && g.kind <= ALEPH_GATE_PHASE && i == 0) ||
+                      (g.kind == ALEPH_GATE_U3) ||
+                      ((g.kind == ALEPH_GATE_CRX || g.kind == ALEPH_GATE_CRY || g.kind == ALEPH_GATE_CRZ) && i == 0);
+    if (used && !std::isfinite(g.params[i])) {
+      set_kind(e, gate_name(g.kind));
+      return fail(e, ALEPH_B200_NON_FINITE_PARAM), 0;
+    }
+  }
+  const double s2 = 0.70710678118654752440, pi4 = 0.78539816339744830962;
+  auto from_pool = [&](uint64_t len) -> const double* {
+    if (!pool || g.data_len != len || g.data_offset + len > pool_len) {
+      set_kind(e, "matrix pool");
+      fail(e, ALEPH_B200_INVALID_ARGUMENT);
+      return nullptr;
+    }
+    return pool + 2 * g.data_offset;
+  };
+  const double t = g.params[0];
+  switch (g.kind) {
+    case ALEPH_GATE_H: m[0][0] = m[0][1] = m[1][0] = Cx{s2, 0}; m[1][1] = Cx{-s2, 0}; return 2;
+    case ALEPH_GATE_X: m[0][1] = m[1][0] = o; return 2;
+    case ALEPH_GATE_Y: m[0][1] = Cx{0, -1}; m[1][0] = Cx{0, 1}; return 2;
+    case ALEPH_GATE_Z: m[0][0] = o; m[1][1] = neg(o); return 2;
+    case ALEPH_GATE_S: m[0][0] = o; m[1][1] = Cx{0, 1}; return 2;
+    case ALEPH_GATE_SDG: m[0][0] = o; m[1][1] = Cx{0, -1}; return 2;
+    case ALEPH_GATE_T: m[0][0] = o; m[1][1] = Cx{std::cos(pi4), std::sin(pi4)}; return 2;
+    case ALEPH_GATE_TDG: m[0][0] = o; m[1][1] = Cx{std::cos(pi4), -std::sin(pi4)}; return 2;
+    case ALEPH_GATE_RX:
+      m[0][0] = m[1][1] = Cx{std::cos(t / 2), 0};
+      m[0][1] = m[1][0] = Cx{0, -std::sin(t / 2)};
+      return 2;
+    case ALEPH_GATE_RY:
+      m[0][0] = m[1][1] = Cx{std::cos(t / 2), 0};
+      m[0][1] = Cx{-std::sin(t / 2), 0};
+      m[1][0] = Cx{std::sin(t / 2), 0};
+      return 2;
+    case ALEPH_GATE_RZ:
+      m[0][0] = Cx{std::cos(t / 2), -std::sin(t / 2)};
+      m[1][1] = Cx{std::cos(t / 2), std::sin(t / 2)};
+      return 2;
+    case ALEPH_GATE_PHASE: m[0][0] = o; m[1][1] = Cx{std::cos(t), std::sin(t)}; return 2;
+    case ALEPH_GATE_U3: {
+      const double f = g.params[1], l = g.params[2];
+      const Cx c{std::cos(t / 2), 0}, s{std::sin(t / 2), 0};
+      m[0][0] = c;
+      m[0][1] = neg(mul(Cx{std::cos(l), std::sin(l)}, s));
+      m[1][0] = mul(Cx{std::cos(f), std::sin(f)}, s);
+      m[1][1] = mul(Cx{std::cos(f + l), std::sin(f + l)}, c);
+      return 2;
+    }
+    case ALEPH_GATE_CNOT: m[0][0] = m[1][1] = m[2][3] = m[3][2] = o; return 4;
+    case ALEPH_GATE_CZ: m[0][0] = m[1][1] = m[2][2] = o; m[3][3] = neg(o); return 4;
+    case ALEPH_GATE_SWAP: m[0][0] = m[1][2] = m[2][1] = m[3][3] = o; return 4;
+    case ALEPH_GATE_ISWAP: m[0][0] = m[3][3] = o; m[1][2] = m[2][1] = Cx{0, 1}; return 4;
+    case ALEPH_GATE_ISWAPDG: m[0][0] = m[3][3] = o; m[1][2] = m[2][1] = Cx{0, -1}; return 4;
+    case ALEPH_GATE_CRX:
+      m[0][0] = m[1][1] = o;
+      m[2][2] = m[3][3] = Cx{std::cos(t / 2), 0};
+      m[2][3] = m[3][2] = Cx{0, -std::sin(t / 2)};
+      return 4;
+    case ALEPH_GATE_CRY:
+      m[0][0] = m[1][1] = o;
+      m[2][2] = m[3][3] = Cx{std::cos(t / 2), 0};
+      m[2][3] = Cx{-std::sin(t / 2), 0};
+      m[3][2] = Cx{std::sin(t / 2), 0};
+      return 4;
+    case ALEPH_GATE_CRZ:
+      m[0][0] = m[1][1] = o;
+      m[2][2] = Cx{std::cos(t / 2), -std::sin(t / 2)};
+      m[3][3] = Cx{std::cos(t / 2), std::sin(t / 2)};
+      return 4;
+    case ALEPH_GATE_TOFFOLI:
+      for (int i = 0; i < 6; ++i) m[i][i] = o;
+      m[6][7] = m[7][6] = o;
+      return 8;
+    case ALEPH_GATE_CCZ:
+      for (int i = 0; i < 7; ++i) m[i][i] = o;
+      m[7][7] = neg(o);
+      return 8;
+    case ALEPH_GATE_UNITARY1Q: {
+      const double* p = from_pool(4);
+      if (!p) return 0;
+      for (int i = 0; i < 4; ++i) m[i / 2][i % 2] = Cx{p[2 * i], p[2 * i + 1]};
+      return 2;
+    }
+    case ALEPH_GATE_UNITARY2Q: {
+      const double* p = from_pool(16);
+      if (!p) return 0;
+      for (int i = 0; i < 16; ++i) m[i / 4][i % 4] = Cx{p[2 * i], p[2 * i + 1]};
+      return 4;
+    }
+    case ALEPH_GATE_UNITARY1QDIAG: {
+      const double* p = from_pool(2);
+      if (!p) return 0;
+      m[0][0] = Cx{p[0], p[1]};
+      m[1][1] = Cx{p[2], p[3]};
+      return 2;
+    }
+    case ALEPH_GATE_UNITARY2QDIAG: {
+      const double* p = from_pool(4);
+      if (!p) return 0;
+      for (int i = 0; i < 4; ++i) m[i][i] = Cx{p[2 * i], p[2 * i + 1]};
+      return 4;
+    }
+  }
+  set_kind(e, gate_name(g.kind));
+  fail(e, ALEPH_B200_UNSUPPORTED_GATE);
+  return 0;
+}
+
+double unitarity_deviation(const Cx* m, int dim) {
+  double worst = 0.0;
+  for (int i = 0; i < dim; ++i)
+    for (int j = 0; j < dim; ++j) {
+      Cx acc{0, 0};
+      for (int c = 0; c < dim; ++c) acc = add(acc, mul(m[i * dim + c], conj(m[j * dim + c])));
+      const Cx d = sub(acc, Cx{i == j ? 1.0 : 0.0, 0});
+      const double dev = std::hypot(d.re, d.im);
+      if (std::isnan(dev)) return NAN;
+      if (dev > worst) worst = dev;
+    }
+  return worst;
+}
+
+bool is_zero(Cx a) { return a.re == 0.0 && a.im == 0.0; }
+bool is_one(Cx a) { return a.re == 1.0 && a.im == 0.0; }
+
+void push_coef(Lowered* L, const Cx* c, int count) {
+  for (int i = 0; i < count; ++i) {
+    L->coef.push_back(c[i].re);
+    L->coef.push_back(c[i].im);
+  }
+}
+
+// Lower a validated dense matrix with MSB-first targets to the cheapest op.
+void lower_matrix(const Cx* m, int dim, const uint32_t* tq, uint64_t ctrl, Lowered* L) {
+  Op& op = L->op;
+  std::memset(&op, 0, sizeof(op));
+  op.ctrl = ctrl;
+  const int k = dim == 2 ? 1 : dim == 4 ? 2 : dim == 8 ? 3 : dim == 16 ? 4 : 5;
+  uint64_t tmask = 0;
+  for (int i = 0; i < k; ++i) tmask |= 1ull << tq[i];
+  bool diag = true;
+  for (int i = 0; i < dim && diag; ++i)
+    for (int j = 0; j < dim; ++j)
+      if (i != j && !is_zero(m[i * dim + j])) {
+        diag = false;
+        break;
+      }
+  if (diag) {
+    // diag(1, ..., 1, c): phase on the all-ones corner
+    bool corner = true;
+    for (int i = 0; i + 1 < dim; ++i)
+      if (!is_one(m[i * dim + i])) corner = false;
+    const Cx c = m[dim * dim - 1];
+    L->nondiag = 0;
+    L->diag = tmask | ctrl;
+    if (corner) {
+      op.mask = tmask | ctrl;
+      op.ctrl = 0;
+      if (c.re == -1.0 && c.im == 0.0) {
+        op.type = OP_NEG;
+      } else {
+        op.type = OP_CPHASE;
+        push_coef(L, &c, 1);
+      }
+      return;
+    }
+    if (k <= 3) {
+      op.type = OP_DIAG;
+      op.nq = (uint8_t)k;
+      for (int i = 0; i < k; ++i) op.q[i] = (uint8_t)tq[i];
+      Cx d[8];
+      for (int i = 0; i < dim; ++i) d[i] = m[i * dim + i];
+      push_coef(L, d, dim);
+      return;
+    }
+  }
+  // controlled blocks: a 2q matrix I (+) U with the MSB as control -> 1q with control
+  if (dim == 4 && is_one(m[0]) && is_zero(m[1]) && is_zero(m[2]) && is_zero(m[3]) && is_zero(m[4]) &&
+      is_one(m[5]) && is_zero(m[6]) && is_zero(m[7]) && is_zero(m[8]) && is_zero(m[9]) && is_zero(m[12]) &&
+      is_zero(m[13])) {
+    const Cx u[4] = {m[10], m[11], m[14], m[15]};
+    uint32_t t1 = tq[1];
+    lower_matrix(u, 2, &t1, ctrl | (1ull << tq[0]), L);
+    return;
+  }
+  // Toffoli / controlled-controlled-U pattern (8x8 identity except the last 2x2 block)
+  if (dim == 8) {
+    bool cc = true;
+    for (int i = 0; i < 8 && cc; ++i)
+      for (int j = 0; j < 8; ++j) {
+        if (i >= 6 && j >= 6) continue;
+        const Cx v = m[i * 8 + j];
+        if (i == j ? !is_one(v) : !is_zero(v)) {
+          cc = false;
+          break;
+        }
+      }
+    if (cc) {
+      const Cx u[4] = {m[54], m[55], m[62], m[63]};
+      uint32_t t2 = tq[2];
+      lower_matrix(u, 2, &t2, ctrl | (1ull << tq[0]) | (1ull << tq[1]), L);
+      return;
+    }
+  }
+  L->nondiag = tmask;
+  L->diag = ctrl;
+  if (dim == 2) {
+    op.nq = 1;
+    op.q[0] = (uint8_t)tq[0];
+    if (is_zero(m[0]) && is_one(m[1]) && is_one(m[2]) && is_zero(m[3])) {
+      op.type = OP_X;
+      return;
+    }
+    op.type = OP_1Q;
+    push_coef(L, m, 4);
+    return;
+  }
+  if (dim == 4) {
+    op.type = OP_2Q;
+    op.nq = 2;
+    op.q[0] = (uint8_t)tq[0];
+    op.q[1] = (uint8_t)tq[1];
+    push_coef(L, m, 16);
+    return;
+  }
+  op.type = OP_KQ;
+  op.nq = (uint8_t)k;
+  for (int i = 0; i < k; ++i) op.q[i] = (uint8_t)tq[i];
+  push_coef(L, m, dim * dim);
+}
+
+}  // namespace
+
+const char* gate_name(uint32_t kind) {
+  static const char* names[] = {"H",   "X",   "Y",   "Z",   "S",     "Sdg",     "T",       "Tdg",
+                                "Rx",  "Ry",  "Rz",  "Phase", "U3",  "Cnot",    "Cz",      "Swap",
+                                "Iswap", "IswapDg", "CRx", "CRy", "CRz", "Toffoli", "Ccz", "Unitary1q",
+                                "Unitary2q", "UnitaryKq", "Unitary1qDiag", "Unitary2qDiag"};
+  if (kind < 28) return names[kind];
+  switch (kind) {
+    case ALEPH_INSTR_MEASURE: return "measure";
+    case ALEPH_INSTR_RESET: return "reset";
+    case ALEPH_INSTR_BARRIER: return "barrier";
+    case ALEPH_INSTR_DIAGONAL_PHASE: return "diagonal_phase";
+    case ALEPH_INSTR_TILED_BLOCK: return "tiled_block";
+  }
+  return "unknown";
+}
+
+int lower_gate(const aleph_b200_instr& g, uint32_t n, const double* pool, uint64_t pool_len, Lowered* L,
+               aleph_b200_error_info* e) {
+  const int expected = arity(g);
+  if (expected < 0) {
+    set_kind(e, gate_name(g.kind));
+    return fail(e, ALEPH_B200_UNSUPPORTED_GATE);
+  }
+  if ((uint32_t)expected != g.num_qubits) {
+    set_kind(e, gate_name(g.kind));
+    e->expected = (uint32_t)expected;
+    e->got = g.num_qubits;
+    return fail(e, ALEPH_B200_ARITY_MISMATCH);
+  }
+  if (g.num_qubits > 8 || g.num_controls > 8) {
+    set_kind(e, "record");
+    return fail(e, ALEPH_B200_INVALID_ARGUMENT);
+  }
+  uint32_t seen[16];
+  uint32_t ns = 0;
+  uint64_t ctrl = 0;
+  for (uint32_t i = 0; i < g.num_qubits + g.num_controls; ++i) {
+    const uint32_t q = i < g.num_qubits ? g.qubits[i] : g.controls[i - g.num_qubits];
+    if (q >= n) {
+      e->qubit = q;
+      e->num_qubits = n;
+      return fail(e, ALEPH_B200_QUBIT_OUT_OF_RANGE);
+    }
+    for (uint32_t j = 0; j < ns; ++j)
+      if (seen[j] == q) {
+        e->qubit = q;
+        return fail(e, ALEPH_B200_DUPLICATE_QUBIT);
+      }
+    seen[ns++] = q;
+    if (i >= g.num_qubits) ctrl |= 1ull << q;
+  }
+  if (g.kind == ALEPH_GATE_UNITARYKQ) {
+    // validate_unitary_kq, crates/aleph-sv/src/validation.rs:113-155
+    const uint32_t k = g.aux;
+    if (k < 2 || k > 5) {
+      set_kind(e, "UnitaryKq width");
+      return fail(e, ALEPH_B200_INVALID_STATE);
+    }
+    if (g.num_controls) {
+      set_kind(e, "controlled UnitaryKq");
+      return fail(e, ALEPH_B200_UNSUPPORTED_GATE);
+    }
+    const uint64_t w = 1ull << k;
+    if (g.data_len != w * w) {
+      set_kind(e, "UnitaryKq length");
+      return fail(e, ALEPH_B200_INVALID_STATE);
+    }
+    if (!pool || g.data_offset + g.data_len > pool_len) {
+      set_kind(e, "matrix pool");
+      return fail(e, ALEPH_B200_INVALID_ARGUMENT);
+    }
+    const Cx* d = reinterpret_cast<const Cx*>(pool + 2 * g.data_offset);
+    for (uint64_t i = 0; i < w * w; ++i)
+      if (!std::isfinite(d[i].re) || !std::isfinite(d[i].im)) {
+        set_kind(e, "UnitaryKq");
+        return fail(e, ALEPH_B200_NON_FINITE_PARAM);
+      }
+    double dev2 = 0.0;
+    for (uint64_t i = 0; i < w; ++i)
+      for (uint64_t j = 0; j <= i; ++j) {
+        Cx s{0, 0};
+        for (uint64_t c = 0; c < w; ++c) s = add(s, mul(d[i * w + c], conj(d[j * w + c])));
+        const Cx df = sub(s, Cx{i == j ? 1.0 : 0.0, 0});
+        const double er = df.re * df.re + df.im * df.im;
+        if (!std::isfinite(er)) {
+          e->value = er;
+          return fail(e, ALEPH_B200_NON_UNITARY_MATRIX);
+        }
+        dev2 = std::max(dev2, er);
+      }
+    if (dev2 > kTol * kTol) {
+      e->value = std::sqrt(dev2);
+      return fail(e, ALEPH_B200_NON_UNITARY_MATRIX);
+    }
+    L->record = 0;
+    lower_matrix(d, (int)w, g.qubits, 0, L);
+    return ALEPH_B200_OK;
+  }
+  Cx m[8][8];
+  const int dim = matrix_of(g, pool, pool_len, m, e);
+  if (dim == 0) return e->status;
+  Cx flat[64];
+  for (int i = 0; i < dim; ++i)
+    for (int j = 0; j < dim; ++j) flat[i * dim + j] = m[i][j];
+  const double dev = unitarity_deviation(flat, dim);
+  if (!std::isfinite(dev) || dev > kTol) {
+    e->value = dev;
+    return fail(e, ALEPH_B200_NON_UNITARY_MATRIX);
+  }
+  lower_matrix(flat, dim, g.qubits, ctrl, L);
+  return ALEPH_B200_OK;
+}
+
+int lower_diagonal_phase(const aleph_b200_phase_term* terms, uint64_t n_terms, const uint64_t* conds, uint64_t n_conds,
+                         Lowered* L, aleph_b200_error_info* e) {
+  std::memset(&L->op, 0, sizeof(L->op));
+  L->op.type = OP_POLY;
+  L->op.aux = (uint32_t)n_terms;
+  uint64_t support = 0;
+  for (uint64_t t = 0; t < n_terms; ++t) {
+    if ((uint64_t)terms[t].cond_offset + terms[t].cond_count > n_conds || (!conds && terms[t].cond_count)) {
+      set_kind(e, "diagonal phase conds");
+      return fail(e, ALEPH_B200_INVALID_ARGUMENT);
+    }
+    L->poly_angle.push_back(terms[t].angle);
+    L->poly_cnt.push_back(terms[t].cond_count);
+    for (uint32_t c = 0; c < terms[t].cond_count; ++c) {
+      L->poly_conds.push_back(conds[terms[t].cond_offset + c]);
+      support |= conds[terms[t].cond_offset + c];
+    }
+  }
+  L->nondiag = 0;
+  L->diag = support;
+  return ALEPH_B200_OK;
+}
+
+// ---------------------------------------------------------------------------
+// planning
+// ---------------------------------------------------------------------------
+namespace {
+
+uint32_t append_op(Plan* P, const Lowered& L, Op op) {
+  op.coef = (uint32_t)(P->coef.size() / 2);
+  P->coef.insert(P->coef.end(), L.coef.begin(), L.coef.end());
+  if (op.type == OP_POLY) {
+    op.mask = P->poly_angle.size();
+    uint32_t off = 0;
+    for (size_t t = 0; t < L.poly_angle.size(); ++t) {
+      P->poly_angle.push_back(L.poly_angle[t]);
+      P->poly_off.push_back((uint32_t)P->poly_conds.size());
+      P->poly_cnt.push_back(L.poly_cnt[t]);
+      for (uint32_t c = 0; c < L.poly_cnt[t]; ++c) P->poly_conds.push_back(L.poly_conds[off + c]);
+      off += L.poly_cnt[t];
+    }
+  }
+  P->ops.push_back(op);
+  return (uint32_t)(P->ops.size() - 1);
+}
+
+// Swap the operand order of a 4x4 matrix (MSB <-> LSB).
+void swap_2q_operands(std::vector<double>& c) {
+  std::vector<double> out(c.size());
+  auto sw = [](int k) { return ((k & 1) << 1) | (k >> 1); };
+  for (int r = 0; r < 4; ++r)
+    for (int cc = 0; cc < 4; ++cc) {
+      const int src = 2 * (4 * r + cc), dst = 2 * (4 * sw(r) + sw(cc));
+      out[dst] = c[src];
+      out[dst + 1] = c[src + 1];
+    }
+  c = out;
+}
+
+void plan_segment_tiles(const std::vector<const Lowered*>& seg, uint32_t n, uint32_t R, Plan* P) {
+  std::vector<const Lowered*> pending = seg;
+  while (!pending.empty()) {
+    const Lowered* head = pending.front();
+    if (head->op.type == OP_KQ) {
+      Pass ps{};
+      ps.kind = PASS_KQ;
+      ps.tile.n = n;
+      ps.tile.op_begin = append_op(P, *head, head->op);
+      ps.tile.op_count = 1;
+      ps.record = head->record;
+      ps.gates = 1;
+      P->passes.push_back(ps);
+      pending.erase(pending.begin());
+      continue;
+    }
+    uint64_t hi = 0;          // register qubits chosen so far
+    uint32_t nhi = 0;
+    uint64_t blocked_full = 0, blocked_diag = 0;
+    std::vector<const Lowered*> take, rest;
+    for (const Lowered* L : pending) {
+      bool ok = !(L->nondiag & (blocked_full | blocked_diag)) && !(L->diag & blocked_full);
+      uint64_t need = 0;
+      if (ok && L->op.type == OP_KQ) ok = false;
+      if (ok && L->nondiag) {
+        need = (L->nondiag >> 5 << 5) & ~hi;
+        if (nhi + (uint32_t)__builtin_popcountll(need) > R) ok = false;
+      }
+      if (ok) {
+        hi |= need;
+        nhi += (uint32_t)__builtin_popcountll(need);
+        take.push_back(L);
+      } else {
+        blocked_full |= L->nondiag;
+        blocked_diag |= L->diag;
+        rest.push_back(L);
+      }
+    }
+    // register qubits: the chosen ones, padded with the lowest unused qubits >= 5
+    TilePass tp{};
+    tp.n = n;
+    tp.R = R;
+    uint32_t j = 0;
+    for (uint32_t q = 5; q < n && j < R; ++q)
+      if ((hi >> q) & 1) tp.hq[j++] = q;
+    for (uint32_t q = 5; q < n && j < R; ++q)
+      if (!((hi >> q) & 1)) {
+        tp.hq[j++] = q;
+        hi |= 1ull << q;
+      }
+    auto slot = [&](uint32_t q) -> uint8_t {
+      if (q < 5) return (uint8_t)q;
+      for (uint32_t i = 0; i < R; ++i)
+        if (tp.hq[i] == q) return (uint8_t)(5 + i);
+      return 255;
+    };
+    tp.op_begin = (uint32_t)P->ops.size();
+    for (const Lowered* L : take) {
+      Op op = L->op;
+      if (op.type == OP_1Q || op.type == OP_X) {
+        op.a = slot(op.q[0]);
+        append_op(P, *L, op);
+      } else if (op.type == OP_2Q) {
+        uint8_t sa = slot(op.q[0]), sb = slot(op.q[1]);
+        if (sa < sb) {
+          Lowered tmp = *L;
+          swap_2q_operands(tmp.coef);
+          std::swap(op.q[0], op.q[1]);
+          op.a = sb;
+          op.b = sa;
+          append_op(P, tmp, op);
+        } else {
+          op.a = sa;
+          op.b = sb;
+          append_op(P, *L, op);
+        }
+      } else {
+        append_op(P, *L, op);
+      }
+    }
+    tp.op_count = (uint32_t)P->ops.size() - tp.op_begin;
+    Pass ps{};
+    ps.kind = PASS_TILE;
+    ps.tile = tp;
+    ps.record = take.empty() ? 0 : take.front()->record;
+    ps.gates = (uint32_t)take.size();
+    P->passes.push_back(ps);
+    pending.swap(rest);
+  }
+}
+
+}  // namespace
+
+int build_plan(const std::vector<Lowered>& ops, uint32_t n, const PlanOptions& o, Plan* P) {
+  std::vector<const Lowered*> seg;
+  auto flush = [&]() {
+    if (seg.empty()) return;
+    if (n <= o.smem_max_n || n < 6) {
+      Pass ps{};
+      ps.kind = PASS_SMEM;
+      ps.tile.n = n;
+      ps.tile.op_begin = (uint32_t)P->ops.size();
+      for (const Lowered* L : seg) append_op(P, *L, L->op);
+      ps.tile.op_count = (uint32_t)P->ops.size() - ps.tile.op_begin;
+      ps.record = seg.front()->record;
+      ps.gates = (uint32_t)seg.size();
+      P->passes.push_back(ps);
+    } else {
+      const uint32_t R = std::min<uint32_t>(std::max<uint32_t>(o.tile_r, 1), std::min<uint32_t>(5, n - 5));
+      plan_segment_tiles(seg, n, R, P);
+    }
+    seg.clear();
+  };
+  for (const Lowered& L : ops) {
+    if (L.is_measure) {
+      flush();
+      Pass ps{};
+      ps.kind = PASS_MEASURE;
+      ps.qubit = L.measure_qubit;
+      ps.record = L.record;
+      P->passes.push_back(ps);
+      ++P->n_measures;
+    } else {
+      seg.push_back(&L);
+    }
+  }
+  flush();
+  return ALEPH_B200_OK;
+}
+
+}  // namespace ab

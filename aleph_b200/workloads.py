@@ -1,0 +1,113 @@
+"""Seeded synthetic workloads with the shapes of the benchmark configurations.
+
+* ``brickwall``: random brickwall — every layer applies a Haar-random SU(2)
+  (from the seed) to each qubit, then CZ on nearest-neighbour pairs (i, i+1),
+  even offsets on even layers and odd offsets on odd layers.
+* ``qft_product``: a random product state (Ry(theta) Rz(phi) per qubit,
+  theta, phi uniform in [0, 2 pi)) followed by the textbook QFT (H plus
+  controlled-phase 2 pi / 2^k on every pair) and the bit-reversal SWAPs.
+* ``qaoa_maxcut``: QAOA on a random 3-regular graph as ``build_qaoa``
+  (crates/aleph-ir/src/ansatz.rs:71-98): H layer, per edge CX Rz(2 gamma) CX,
+  Rx(2 beta) mixer, p layers.
+
+All data are synthetic (generated here from seeds); no benchmark suite items
+are reproduced.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from . import circuit as C
+
+
+def haar_su2(rng: np.random.Generator) -> np.ndarray:
+    """Haar-random SU(2): QR of a complex Gaussian matrix, phase-fixed, det = 1."""
+    z = (rng.standard_normal((2, 2)) + 1j * rng.standard_normal((2, 2))) / math.sqrt(2.0)
+    q, r = np.linalg.qr(z)
+    d = np.diag(r)
+    q = q * (d / np.abs(d))
+    q = q / np.sqrt(np.linalg.det(q))
+    return q
+
+
+def brickwall(n: int, depth: int, seed: int = 0) -> C.Circuit:
+    rng = np.random.default_rng(seed)
+    c = C.Circuit(n)
+    for layer in range(depth):
+        for q in range(n):
+            c.add(C.Unitary1q(haar_su2(rng)), [q])
+        for q in range(layer % 2, n - 1, 2):
+            c.add(C.Cz(), [q, q + 1])
+    return c
+
+
+def qft_product(n: int, seed: int = 0, swaps: bool = True) -> C.Circuit:
+    rng = np.random.default_rng(seed)
+    c = C.Circuit(n)
+    for q in range(n):
+        th, ph = rng.uniform(0.0, 2.0 * math.pi, size=2)
+        c.add(C.Ry(th), [q])
+        c.add(C.Rz(ph), [q])
+    for j in range(n - 1, -1, -1):
+        c.add(C.H(), [j])
+        for k in range(j - 1, -1, -1):
+            # controlled phase 2*pi / 2^(j-k+1), control k, target j
+            c.add(C.Phase(2.0 * math.pi / (2 ** (j - k + 1))), [j], controls=[k])
+    if swaps:
+        for q in range(n // 2):
+            c.add(C.Swap(), [q, n - 1 - q])
+    return c
+
+
+def random_3_regular(n: int, rng: np.random.Generator) -> list[tuple[int, int]]:
+    """Pairing model with rejection: a uniformly random simple 3-regular graph."""
+    if (3 * n) % 2:
+        raise ValueError("3-regular graphs need an even vertex count")
+    while True:
+        stubs = np.repeat(np.arange(n), 3)
+        rng.shuffle(stubs)
+        edges = set()
+        ok = True
+        for a, b in zip(stubs[0::2], stubs[1::2]):
+            a, b = int(a), int(b)
+            if a == b or (min(a, b), max(a, b)) in edges:
+                ok = False
+                break
+            edges.add((min(a, b), max(a, b)))
+        if ok:
+            return sorted(edges)
+
+
+def qaoa_maxcut(n: int, edges, gammas, betas) -> C.Circuit:
+    c = C.Circuit(n)
+    for q in range(n):
+        c.add(C.H(), [q])
+    for g, b in zip(gammas, betas):
+        for (i, j) in edges:
+            c.add(C.Cnot(), [i, j])
+            c.add(C.Rz(2.0 * g), [j])
+            c.add(C.Cnot(), [i, j])
+        for q in range(n):
+            c.add(C.Rx(2.0 * b), [q])
+    return c
+
+
+def maxcut_terms(edges):
+    """<C> = sum_edges 1/2 (1 - <Z_i Z_j>) (crates/aleph-ir/src/ansatz.rs:105-117)."""
+    return [((i, "Z"), (j, "Z")) for (i, j) in edges]
+
+
+def splitmix64_words(seed: int, count: int) -> np.ndarray:
+    """Deterministic u64 variates (splitmix64) shared by the engine and the oracle in tests."""
+    out = np.empty(count, dtype=np.uint64)
+    x = seed & 0xFFFFFFFFFFFFFFFF
+    M = 0xFFFFFFFFFFFFFFFF
+    for i in range(count):
+        x = (x + 0x9E3779B97F4A7C15) & M
+        z = x
+        z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & M
+        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & M
+        out[i] = z ^ (z >> 31)
+    return out

@@ -1,0 +1,263 @@
+/*
+ * aleph_b200.h — C ABI of the B200-native dense state-vector engine.
+ *
+ * The entry points mirror aleph's `Backend` trait
+ * (crates/aleph-backend/src/lib.rs:86-163) so that a host binding (Rust FFI,
+ * ctypes, pybind) can stand in for the `sv` / `cuda` backends:
+ *
+ *   Backend::allocate             -> aleph_b200_allocate
+ *   Backend::apply_gate           -> aleph_b200_apply_gate
+ *   Backend::apply_diagonal_phase -> aleph_b200_apply_diagonal_phase
+ *   Backend::apply_tiled_block    -> aleph_b200_apply_gate_stream (TILED_BLOCK record)
+ *   Backend::unpermute_state      -> aleph_b200_unpermute
+ *   Backend::measure              -> aleph_b200_measure
+ *   Backend::sample               -> aleph_b200_sample / aleph_b200_sample_seeded
+ *   Backend::expectation_value    -> aleph_b200_expectation
+ *   Backend::probabilities        -> aleph_b200_probabilities
+ *   run / run_with_outcomes       -> aleph_b200_apply_gate_stream
+ *     (crates/aleph-backend/src/lib.rs:182-245)
+ *
+ * Every function returns an aleph_b200_status (0 = OK). Non-zero codes map
+ * 1:1 onto the variants of `BackendError` (crates/aleph-backend/src/lib.rs:22-74);
+ * the message and payload of the last error are available through
+ * aleph_b200_last_error / aleph_b200_last_error_info. The engine never aborts
+ * the process and never traps the GPU.
+ *
+ * Plain C types only: pointers, sizes, POD structs. No framework types.
+ */
+#ifndef ALEPH_B200_H
+#define ALEPH_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ALEPH_B200_ABI_VERSION 1
+
+/* ---- status codes: BackendError variants (crates/aleph-backend/src/lib.rs:22-74) ---- */
+typedef enum aleph_b200_status {
+  ALEPH_B200_OK = 0,
+  ALEPH_B200_DEVICE_FAILURE = 1,          /* DeviceFailure(String)                 */
+  ALEPH_B200_QUBIT_OUT_OF_RANGE = 2,      /* QubitOutOfRange { qubit, num_qubits } */
+  ALEPH_B200_DUPLICATE_QUBIT = 3,         /* DuplicateQubit { qubit }              */
+  ALEPH_B200_ARITY_MISMATCH = 4,          /* ArityMismatch { kind, expected, got } */
+  ALEPH_B200_UNSUPPORTED_GATE = 5,        /* UnsupportedGate { kind }              */
+  ALEPH_B200_UNSUPPORTED_INSTRUCTION = 6, /* UnsupportedInstruction { kind }       */
+  ALEPH_B200_SYMBOLIC_PARAM = 7,          /* SymbolicParam                         */
+  ALEPH_B200_NON_FINITE_PARAM = 8,        /* NonFiniteParam { kind }               */
+  ALEPH_B200_NON_UNITARY_MATRIX = 9,      /* NonUnitaryMatrix { deviation }        */
+  ALEPH_B200_EMPTY_CIRCUIT = 10,          /* EmptyCircuit                          */
+  ALEPH_B200_DEGENERATE_MEASUREMENT = 11, /* DegenerateMeasurement { qubit, p }    */
+  ALEPH_B200_TOO_MANY_QUBITS = 12,        /* TooManyQubits { requested, limit }    */
+  ALEPH_B200_INVALID_PAULI_STRING = 13,   /* InvalidPauliString { reason }         */
+  ALEPH_B200_INVALID_STATE = 14,          /* InvalidState { reason }               */
+  ALEPH_B200_OPTIMIZATION = 15,           /* Optimization(PassError)               */
+  ALEPH_B200_INVALID_ARGUMENT = 16        /* ABI misuse: null pointer, bad enum    */
+} aleph_b200_status;
+
+/* ---- gate kinds: the `Gate` enum, declaration order (crates/aleph-core/src/gate/kinds.rs:12-107) ---- */
+typedef enum aleph_b200_kind {
+  ALEPH_GATE_H = 0,
+  ALEPH_GATE_X = 1,
+  ALEPH_GATE_Y = 2,
+  ALEPH_GATE_Z = 3,
+  ALEPH_GATE_S = 4,
+  ALEPH_GATE_SDG = 5,
+  ALEPH_GATE_T = 6,
+  ALEPH_GATE_TDG = 7,
+  ALEPH_GATE_RX = 8,         /* params[0] = theta                       */
+  ALEPH_GATE_RY = 9,
+  ALEPH_GATE_RZ = 10,
+  ALEPH_GATE_PHASE = 11,
+  ALEPH_GATE_U3 = 12,        /* params = (theta, phi, lambda)           */
+  ALEPH_GATE_CNOT = 13,      /* qubits = [control, target]              */
+  ALEPH_GATE_CZ = 14,
+  ALEPH_GATE_SWAP = 15,
+  ALEPH_GATE_ISWAP = 16,
+  ALEPH_GATE_ISWAPDG = 17,
+  ALEPH_GATE_CRX = 18,       /* qubits = [control, target]              */
+  ALEPH_GATE_CRY = 19,
+  ALEPH_GATE_CRZ = 20,
+  ALEPH_GATE_TOFFOLI = 21,   /* qubits = [c0, c1, target]               */
+  ALEPH_GATE_CCZ = 22,
+  ALEPH_GATE_UNITARY1Q = 23, /* 4 complex (row-major) at data_offset    */
+  ALEPH_GATE_UNITARY2Q = 24, /* 16 complex, qubits[0] = matrix MSB      */
+  ALEPH_GATE_UNITARYKQ = 25, /* aux = k (2..5), 4^k complex, MSB-first  */
+  ALEPH_GATE_UNITARY1QDIAG = 26, /* 2 complex diagonal entries          */
+  ALEPH_GATE_UNITARY2QDIAG = 27, /* 4 complex diagonal entries          */
+  /* non-gate instructions (crates/aleph-ir/src/instruction.rs:13-34) */
+  ALEPH_INSTR_MEASURE = 100,        /* qubits[0] = qubit, aux = clbit           */
+  ALEPH_INSTR_RESET = 101,          /* rejected: UnsupportedInstruction "reset" */
+  ALEPH_INSTR_BARRIER = 102,        /* no-op                                    */
+  ALEPH_INSTR_DIAGONAL_PHASE = 103, /* terms [data_offset, data_offset+data_len) */
+  ALEPH_INSTR_TILED_BLOCK = 104     /* aux = tile_bits; the next data_len records are its gates */
+} aleph_b200_kind;
+
+/* One instruction of the flattened aleph-ir gate stream. `GateInstance`
+ * (crates/aleph-core/src/gate/instance.rs:56-61) is {gate, qubits, controls};
+ * qubits are in the gate's operand order (qubits[0] = matrix MSB). */
+typedef struct aleph_b200_instr {
+  uint32_t kind;          /* aleph_b200_kind                                        */
+  uint32_t num_qubits;    /* entries used in qubits[]                               */
+  uint32_t num_controls;  /* entries used in controls[]                             */
+  uint32_t aux;           /* MEASURE: clbit; UNITARYKQ: k; TILED_BLOCK: tile_bits   */
+  uint32_t qubits[8];
+  uint32_t controls[8];
+  double params[3];
+  uint64_t data_offset;   /* matrix pool offset in complex elements / first term    */
+  uint64_t data_len;      /* complex elements / terms / TILED_BLOCK gate count      */
+} aleph_b200_instr;
+
+/* One `PhaseTerm` (crates/aleph-ir/src/diagonal_phase.rs:20-26): adds `angle`
+ * to the phase of |x> when parity(mask & x) is odd for every mask in
+ * cond_pool[cond_offset .. cond_offset + cond_count). */
+typedef struct aleph_b200_phase_term {
+  double angle;
+  uint32_t cond_offset;
+  uint32_t cond_count;
+} aleph_b200_phase_term;
+
+/* Side tables of a gate stream. Any pointer may be NULL when its count is 0. */
+typedef struct aleph_b200_pools {
+  const double* matrix_pool;           /* interleaved (re, im) complex */
+  uint64_t matrix_pool_len;            /* in complex elements          */
+  const aleph_b200_phase_term* terms;
+  uint64_t n_terms;
+  const uint64_t* cond_pool;
+  uint64_t n_conds;
+} aleph_b200_pools;
+
+typedef enum aleph_b200_precision {
+  ALEPH_B200_F64 = 0,  /* complex128 state, FP64 arithmetic                         */
+  ALEPH_B200_F32 = 1,  /* complex64 state, FP32 CUDA-core arithmetic                */
+  ALEPH_B200_TC32 = 2  /* complex64 state, fused 6-qubit blocks on tcgen05 tensor
+                          cores with split-BF16x3 operands and FP32 accumulation   */
+} aleph_b200_precision;
+
+typedef enum aleph_b200_sample_mode {
+  /* one uint64 word per shot, Vose alias table
+     (crates/aleph-sv/src/sampling.rs:93-198); the reference's shots >= 2 path */
+  ALEPH_B200_SAMPLE_ALIAS = 0,
+  /* one double in [0,1) per shot, inverse CDF with cumulative_index semantics
+     (crates/aleph-sv/src/sampling.rs:59-91); the reference's shots <= 1 path */
+  ALEPH_B200_SAMPLE_CUMULATIVE = 1,
+  /* the reference's own rule: ALIAS when shots >= 2, CUMULATIVE otherwise
+     (crates/aleph-sv/src/measure.rs:109-124); `variates` then holds uint64
+     words for ALIAS, or one double for CUMULATIVE */
+  ALEPH_B200_SAMPLE_AUTO = 2
+} aleph_b200_sample_mode;
+
+typedef enum aleph_b200_pauli { ALEPH_PAULI_I = 0, ALEPH_PAULI_X = 1, ALEPH_PAULI_Y = 2, ALEPH_PAULI_Z = 3 } aleph_b200_pauli;
+
+typedef struct aleph_b200_handle aleph_b200_handle;
+typedef struct aleph_b200_state aleph_b200_state;
+
+/* Payload of the last error (fields not used by a variant are zero). */
+typedef struct aleph_b200_error_info {
+  int32_t status;
+  uint32_t qubit;       /* QubitOutOfRange, DuplicateQubit, DegenerateMeasurement */
+  uint32_t num_qubits;  /* QubitOutOfRange                                        */
+  uint32_t expected;    /* ArityMismatch                                          */
+  uint32_t got;         /* ArityMismatch                                          */
+  uint32_t requested;   /* TooManyQubits                                          */
+  uint32_t limit;       /* TooManyQubits                                          */
+  uint32_t instruction; /* index of the failing record in a gate stream           */
+  double value;         /* NonUnitaryMatrix deviation / DegenerateMeasurement p   */
+  char kind[32];        /* gate / instruction name (Gate::name, kinds.rs:156-186) */
+} aleph_b200_error_info;
+
+/* ---- lifecycle ---- */
+
+/* Replaces NaiveSvBackend::with_seed / CudaSvBackend::new
+ * (crates/aleph-sv/src/backend.rs:36-42, crates/aleph-cuda/src/sv/backend.rs:94-129).
+ * Binds `device`, creates one stream and the per-handle RNG seeded with `seed`. */
+int aleph_b200_create(uint64_t seed, int device, int precision, aleph_b200_handle** out);
+int aleph_b200_destroy(aleph_b200_handle* h);
+/* Qubit cap of `allocate` (MAX_NAIVE_QUBITS analogue, backend.rs:11,46-49).
+ * Default: 33 (F64) / 34 (F32, TC32). */
+int aleph_b200_set_qubit_cap(aleph_b200_handle* h, uint32_t cap);
+
+/* ---- Backend::allocate (crates/aleph-sv/src/backend.rs:61-72): |0...0> ---- */
+int aleph_b200_allocate(aleph_b200_handle* h, uint32_t num_qubits, aleph_b200_state** out);
+int aleph_b200_free_state(aleph_b200_handle* h, aleph_b200_state* st);
+int aleph_b200_num_qubits(const aleph_b200_state* st, uint32_t* out);
+
+/* ---- Backend::apply_gate (crates/aleph-sv/src/backend.rs:74-152) ---- */
+int aleph_b200_apply_gate(aleph_b200_handle* h, aleph_b200_state* st, const aleph_b200_instr* gate,
+                          const double* matrix_pool, uint64_t matrix_pool_len);
+
+/* ---- run_with_outcomes (crates/aleph-backend/src/lib.rs:211-245) ----
+ * Validates the whole stream first (first invalid record -> its error, state
+ * untouched), then plans and launches it. MEASURE records draw one uniform
+ * from `measure_uniforms` per non-degenerate measurement, in order; with
+ * measure_uniforms == NULL the handle's RNG supplies them. Outcomes (0/1) are
+ * written to `outcomes` in record order; `*n_outcomes` receives their count. */
+int aleph_b200_apply_gate_stream(aleph_b200_handle* h, aleph_b200_state* st, const aleph_b200_instr* instrs,
+                                 uint64_t count, const aleph_b200_pools* pools, const double* measure_uniforms,
+                                 uint64_t n_uniforms, uint8_t* outcomes, uint64_t outcomes_cap,
+                                 uint64_t* n_outcomes);
+
+/* ---- Backend::apply_diagonal_phase (crates/aleph-sv/src/kernels/diagonal_phase.rs:74-97) ---- */
+int aleph_b200_apply_diagonal_phase(aleph_b200_handle* h, aleph_b200_state* st, const aleph_b200_phase_term* terms,
+                                    uint64_t n_terms, const uint64_t* cond_pool, uint64_t n_conds);
+
+/* ---- Backend::unpermute_state (crates/aleph-core/src/perm.rs:25-40): perm[logical] = physical ---- */
+int aleph_b200_unpermute(aleph_b200_handle* h, aleph_b200_state* st, const uint32_t* perm, uint32_t n);
+
+/* ---- Backend::measure (crates/aleph-sv/src/measure.rs:41-102) ----
+ * `u` is the uniform consumed when both branches are non-degenerate; pass a
+ * negative value to draw it from the handle's RNG. *consumed = 1 if it was used. */
+int aleph_b200_measure(aleph_b200_handle* h, aleph_b200_state* st, uint32_t qubit, double u, int* outcome,
+                       int* consumed);
+
+/* ---- Backend::sample (crates/aleph-sv/src/measure.rs:109-148) ----
+ * `variates`: uint64 words (ALIAS) or doubles in [0,1) (CUMULATIVE), one per shot. */
+int aleph_b200_sample(aleph_b200_handle* h, aleph_b200_state* st, uint32_t shots, int mode, const void* variates,
+                      uint64_t* out);
+/* Same, with variates drawn from the handle's RNG (AUTO rule). */
+int aleph_b200_sample_seeded(aleph_b200_handle* h, aleph_b200_state* st, uint32_t shots, uint64_t* out);
+
+/* ---- Backend::expectation_value (crates/aleph-sv/src/measure.rs:155-233) ---- */
+int aleph_b200_expectation(aleph_b200_handle* h, aleph_b200_state* st, const uint32_t* qubits,
+                           const uint8_t* paulis, uint32_t n_terms, double coefficient, double* out);
+
+/* ---- Backend::probabilities (crates/aleph-sv/src/measure.rs:239-273): qubits[0] = LSB of the output index ---- */
+int aleph_b200_probabilities(aleph_b200_handle* h, aleph_b200_state* st, const uint32_t* qubits, uint32_t k,
+                             double* out);
+
+/* ---- state access (RunResult.statevector(), crates/aleph-py/src/run.rs:71-101) ----
+ * Interleaved (re, im) doubles, 2 * 2^n values; FP32 states are widened. */
+int aleph_b200_get_amplitudes(aleph_b200_handle* h, aleph_b200_state* st, double* out);
+int aleph_b200_set_amplitudes(aleph_b200_handle* h, aleph_b200_state* st, const double* in);
+/* FP64 sum of |a_i|^2 on the device. */
+int aleph_b200_norm_sqr(aleph_b200_handle* h, aleph_b200_state* st, double* out);
+
+/* ---- stream / errors ---- */
+int aleph_b200_synchronize(aleph_b200_handle* h);
+int aleph_b200_last_error(const aleph_b200_handle* h, char* buf, uint64_t len);
+int aleph_b200_last_error_info(const aleph_b200_handle* h, aleph_b200_error_info* out);
+
+/* ---- planner tuning (the autotuner's knobs) ----
+ * keys: "tile_r" (register qubits per warp tile, 1..5), "smem_max_n" (states
+ * with n <= this run as one shared-memory pass, 0..12). */
+int aleph_b200_set_tuning(aleph_b200_handle* h, const char* key, int64_t value);
+
+/* ---- launch statistics (execution_counters, crates/aleph-cuda/src/execution.rs:145-165) ---- */
+typedef struct aleph_b200_stats {
+  uint64_t kernel_launches;   /* engine kernels launched by this handle            */
+  uint64_t passes;            /* full-state HBM passes issued by gate streams       */
+  uint64_t tile_passes;       /* of which CUDA-core tile passes                     */
+  uint64_t block_passes;      /* of which tensor-core dense-block passes            */
+  uint64_t gates_planned;     /* gates consumed by the planner                      */
+  double algorithmic_bytes;   /* sum of (amplitudes read + written) * bytes/amp     */
+} aleph_b200_stats;
+int aleph_b200_get_stats(const aleph_b200_handle* h, aleph_b200_stats* out);
+int aleph_b200_reset_stats(aleph_b200_handle* h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ALEPH_B200_H */

@@ -1,0 +1,167 @@
+"""ctypes binding of the CPU oracle (oracle/sv_oracle.cpp). TEST INFRASTRUCTURE.
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline /
+reference arm import this module. It restates the reference's FP64 CPU
+``sv`` backend and is the checker of the B200 engine, never its fallback.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+from aleph_b200 import abi
+from aleph_b200.circuit import flatten
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "_build" / "libsv_oracle.so"
+_lib = None
+
+
+def build() -> Path:
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+    return LIB
+
+
+def lib() -> ct.CDLL:
+    global _lib
+    if _lib is None:
+        if not LIB.exists():
+            build()
+        L = ct.CDLL(str(LIB))
+        D = ct.POINTER(ct.c_double)
+        U64 = ct.POINTER(ct.c_uint64)
+        U32 = ct.POINTER(ct.c_uint32)
+        sig = {
+            "orc_last_error": ([ct.POINTER(abi.ErrorInfo)], ct.c_int),
+            "orc_init": ([D, ct.c_uint32], ct.c_int),
+            "orc_apply_gate": ([D, ct.c_uint32, ct.POINTER(abi.Instr), D, ct.c_uint64], ct.c_int),
+            "orc_gate_matrix": ([ct.POINTER(abi.Instr), D, ct.c_uint64, D, ct.POINTER(ct.c_int)], ct.c_int),
+            "orc_apply_diagonal_phase": ([D, ct.c_uint32, ct.POINTER(abi.PhaseTerm), ct.c_uint64, U64, ct.c_uint64], ct.c_int),
+            "orc_unpermute": ([D, ct.c_uint32, U32], ct.c_int),
+            "orc_measure": ([D, ct.c_uint32, ct.c_uint32, ct.c_double, ct.POINTER(ct.c_int), ct.POINTER(ct.c_int)], ct.c_int),
+            "orc_sample_cumulative": ([D, ct.c_uint32, ct.c_uint32, D, U64], ct.c_int),
+            "orc_sample_alias": ([D, ct.c_uint32, ct.c_uint32, U64, U64], ct.c_int),
+            "orc_alias_table": ([D, ct.c_uint64, D, U32], ct.c_int),
+            "orc_expectation": ([D, ct.c_uint32, U32, ct.POINTER(ct.c_uint8), ct.c_uint32, ct.c_double, D], ct.c_int),
+            "orc_probabilities": ([D, ct.c_uint32, U32, ct.c_uint32, D], ct.c_int),
+            "orc_norm_sqr": ([D, ct.c_uint32, D], ct.c_int),
+            "orc_run_stream": ([D, ct.c_uint32, ct.POINTER(abi.Instr), ct.c_uint64, ct.POINTER(abi.Pools), D,
+                                ct.c_uint64, ct.POINTER(ct.c_uint8), ct.c_uint64, U64, U64], ct.c_int),
+        }
+        for k, (a, r) in sig.items():
+            f = getattr(L, k)
+            f.argtypes = a
+            f.restype = r
+        _lib = L
+    return _lib
+
+
+class OracleError(Exception):
+    def __init__(self, status, info):
+        self.status = status
+        self.info = info
+        super().__init__(f"{abi.STATUS_NAMES.get(status, status)}: {info.kind.decode(errors='replace')}")
+
+
+def _dp(a):
+    return a.ctypes.data_as(ct.POINTER(ct.c_double))
+
+
+def _check(st):
+    if st != 0:
+        info = abi.ErrorInfo()
+        lib().orc_last_error(ct.byref(info))
+        raise OracleError(st, info)
+
+
+def zero_state(n: int) -> np.ndarray:
+    s = np.zeros(1 << n, dtype=np.complex128)
+    s[0] = 1.0
+    return s
+
+
+def run(n: int, instructions, uniforms=None, state: np.ndarray | None = None):
+    """run_with_outcomes on the oracle: returns (state, outcomes)."""
+    flat = flatten(instructions)
+    psi = zero_state(n) if state is None else np.array(state, dtype=np.complex128, copy=True)
+    u = np.ascontiguousarray(np.asarray(uniforms if uniforms is not None else [], dtype=np.float64))
+    outs = (ct.c_uint8 * max(1, flat.n))()
+    nout = ct.c_uint64()
+    failed = ct.c_uint64()
+    st = lib().orc_run_stream(_dp(psi), n, flat.instrs, flat.n, ct.byref(flat.pools),
+                              _dp(u) if u.size else None, u.size, outs, flat.n, ct.byref(nout), ct.byref(failed))
+    _check(st)
+    return psi, [int(outs[i]) for i in range(nout.value)]
+
+
+def sample_alias(psi: np.ndarray, words) -> np.ndarray:
+    psi = np.ascontiguousarray(psi, dtype=np.complex128)
+    n = psi.size.bit_length() - 1
+    w = np.ascontiguousarray(np.asarray(words, dtype=np.uint64))
+    out = np.zeros(w.size, dtype=np.uint64)
+    _check(lib().orc_sample_alias(_dp(psi), n, w.size, w.ctypes.data_as(ct.POINTER(ct.c_uint64)),
+                                  out.ctypes.data_as(ct.POINTER(ct.c_uint64))))
+    return out
+
+
+def sample_cumulative(psi: np.ndarray, uniforms) -> np.ndarray:
+    psi = np.ascontiguousarray(psi, dtype=np.complex128)
+    n = psi.size.bit_length() - 1
+    u = np.ascontiguousarray(np.asarray(uniforms, dtype=np.float64))
+    out = np.zeros(u.size, dtype=np.uint64)
+    _check(lib().orc_sample_cumulative(_dp(psi), n, u.size, _dp(u), out.ctypes.data_as(ct.POINTER(ct.c_uint64))))
+    return out
+
+
+def alias_table(probs):
+    p = np.ascontiguousarray(np.asarray(probs, dtype=np.float64))
+    prob = np.zeros_like(p)
+    alias = np.zeros(p.size, dtype=np.uint32)
+    _check(lib().orc_alias_table(_dp(p), p.size, _dp(prob), alias.ctypes.data_as(ct.POINTER(ct.c_uint32))))
+    return prob, alias
+
+
+def measure(psi: np.ndarray, qubit: int, u: float):
+    n = psi.size.bit_length() - 1
+    o, c = ct.c_int(), ct.c_int()
+    _check(lib().orc_measure(_dp(psi), n, qubit, u, ct.byref(o), ct.byref(c)))
+    return o.value, c.value
+
+
+def expectation(psi: np.ndarray, terms, coefficient=1.0) -> float:
+    psi = np.ascontiguousarray(psi, dtype=np.complex128)
+    n = psi.size.bit_length() - 1
+    qs = (ct.c_uint32 * max(1, len(terms)))(*[q for q, _ in terms])
+    ps = (ct.c_uint8 * max(1, len(terms)))(*[abi.PAULI[p] for _, p in terms])
+    out = ct.c_double()
+    _check(lib().orc_expectation(_dp(psi), n, qs, ps, len(terms), coefficient, ct.byref(out)))
+    return out.value
+
+
+def probabilities(psi: np.ndarray, qubits) -> np.ndarray:
+    psi = np.ascontiguousarray(psi, dtype=np.complex128)
+    n = psi.size.bit_length() - 1
+    qs = (ct.c_uint32 * max(1, len(qubits)))(*qubits)
+    out = np.zeros(1 << len(qubits), dtype=np.float64)
+    _check(lib().orc_probabilities(_dp(psi), n, qs, len(qubits), _dp(out)))
+    return out
+
+
+def unpermute(psi: np.ndarray, perm) -> np.ndarray:
+    psi = np.array(psi, dtype=np.complex128, copy=True)
+    n = psi.size.bit_length() - 1
+    p = (ct.c_uint32 * n)(*perm)
+    _check(lib().orc_unpermute(_dp(psi), n, p))
+    return psi
+
+
+def gate_matrix(inst) -> np.ndarray:
+    flat = flatten([inst])
+    out = np.zeros(128, dtype=np.float64)
+    dim = ct.c_int()
+    _check(lib().orc_gate_matrix(flat.instrs, flat.matrix_ptr, flat.matrix.size // 2, _dp(out), ct.byref(dim)))
+    d = dim.value
+    return (out[0:2 * d * d:2] + 1j * out[1:2 * d * d:2]).reshape(d, d)

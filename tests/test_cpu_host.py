@@ -1,0 +1,171 @@
+"""CPU-side tests: the C-ABI library loads and exports every declared
+symbol, the host-side stream flattening, the workload generators, and
+oracle known-answer tests from the reference's own unit tests."""
+import ctypes as ct
+import math
+
+import numpy as np
+import pytest
+
+from aleph_b200 import abi
+from aleph_b200 import circuit as C
+from aleph_b200 import workloads
+from oracle import oracle
+
+
+def test_library_exports_every_declared_symbol():
+    lib = abi.load_library()
+    declared = abi.declared_symbols()
+    assert len(declared) >= 24
+    for name in declared:
+        assert hasattr(lib, name), name
+        assert name in abi._SIGNATURES, f"{name} has no ctypes signature"
+
+
+def test_create_without_gpu_reports_device_failure():
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("GPU present")
+    lib = abi.load_library()
+    h = ct.c_void_p()
+    assert lib.aleph_b200_create(0, 0, 0, ct.byref(h)) == abi.DEVICE_FAILURE
+    assert lib.aleph_b200_create(0, 0, 7, ct.byref(h)) == abi.INVALID_ARGUMENT
+
+
+def test_record_layout_matches_header():
+    # struct aleph_b200_instr: 4*4 + 8*4 + 8*4 + 3*8 + 8 + 8 bytes
+    assert ct.sizeof(abi.Instr) == 120
+    assert ct.sizeof(abi.PhaseTerm) == 16
+    assert ct.sizeof(abi.ErrorInfo) == 4 * 8 + 8 + 32
+
+
+def test_flatten_roundtrip():
+    c = C.Circuit(4)
+    c.add(C.U3(0.1, 0.2, 0.3), [2]).add(C.Unitary2q(np.eye(4)), [0, 3], [1]).measure(2, 5)
+    c.instructions.append(C.DiagonalPhase(4, [C.PhaseTerm((0b11, 0b100), 0.5), C.PhaseTerm((), 0.1)]))
+    c.instructions.append(C.TiledBlock([C.GateInstance(C.H(), [0])], 15))
+    f = C.flatten(c)
+    assert f.n == 6
+    assert f.instrs[0].kind == abi.KIND["U3"] and list(f.instrs[0].params) == [0.1, 0.2, 0.3]
+    assert f.instrs[1].num_controls == 1 and f.instrs[1].controls[0] == 1 and f.instrs[1].data_len == 16
+    assert f.instrs[2].kind == abi.INSTR_MEASURE and f.instrs[2].aux == 5
+    assert f.instrs[3].kind == abi.INSTR_DIAGONAL_PHASE and f.instrs[3].data_len == 2
+    assert list(f.conds) == [0b11, 0b100]
+    assert f.instrs[4].kind == abi.INSTR_TILED_BLOCK and f.instrs[4].data_len == 1
+    assert f.instrs[5].kind == abi.KIND["H"]
+
+
+def test_haar_su2_is_special_unitary():
+    rng = np.random.default_rng(0)
+    for _ in range(20):
+        u = workloads.haar_su2(rng)
+        assert np.allclose(u @ u.conj().T, np.eye(2), atol=1e-14)
+        assert abs(np.linalg.det(u) - 1) < 1e-14
+
+
+def test_brickwall_shape():
+    c = workloads.brickwall(20, 20, seed=0)
+    assert c.gate_count() == 20 * 20 + 10 * 10 + 10 * 9
+
+
+def test_random_3_regular():
+    rng = np.random.default_rng(1)
+    for n in (12, 16, 24):
+        e = workloads.random_3_regular(n, rng)
+        deg = np.zeros(n, int)
+        for a, b in e:
+            deg[a] += 1
+            deg[b] += 1
+        assert (deg == 3).all() and len(set(e)) == len(e)
+
+
+# ---- oracle known-answer tests (reference unit tests) -------------------------
+def test_oracle_exact_inverse_boundaries():
+    # Boundary known-answer test in the shape of the reference GPU sampler's
+    # (crates/aleph-cuda/src/sv/sampling.rs:466-527: mass on indices 1, 255,
+    # 256, 511), with exactly representable probabilities so the expected
+    # outcomes of cumulative_index (strict `target < cumulative`, zero bins
+    # skipped, crates/aleph-sv/src/sampling.rs:59-81) are known in closed form.
+    psi = np.zeros(512, dtype=np.complex128)
+    psi[[1, 255, 256, 511]] = 0.5
+    u = [0.0, np.nextafter(0.25, 0), 0.25, np.nextafter(0.5, 0), 0.5, 0.75, np.nextafter(1.0, 0)]
+    assert list(oracle.sample_cumulative(psi, u)) == [1, 1, 255, 255, 256, 511, 511]
+
+
+def test_oracle_cumulative_boundaries():
+    # crates/aleph-sv/src/sampling.rs:205-219: strict comparison skips zero
+    # bins and an exact boundary moves to the next positive bin
+    psi = np.array([0, 0.5, 0, 0.5, 0.5, 0, 0.5, 0], dtype=np.complex128)
+    assert oracle.sample_cumulative(psi, [0.25])[0] == 3
+    assert oracle.sample_cumulative(psi, [0.0])[0] == 1
+    psi = np.array([0, 1, 0, 0], dtype=np.complex128)
+    assert oracle.sample_cumulative(psi, [0.0])[0] == 1
+    assert oracle.sample_cumulative(psi, [np.nextafter(1.0, 0)])[0] == 1
+
+
+def test_oracle_alias_table_reconstructs_distribution():
+    rng = np.random.default_rng(2)
+    p = rng.random(64)
+    p /= p.sum()
+    prob, alias = oracle.alias_table(p)
+    n = p.size
+    recon = prob.copy()
+    for j in range(n):
+        if alias[j] != j:
+            recon[alias[j]] += 1.0 - prob[j]
+    assert np.allclose(recon / n, p, atol=1e-12)
+
+
+def test_oracle_alias_uniform_self_aliased():
+    prob, alias = oracle.alias_table(np.full(16, 1 / 16))
+    assert (prob == 1.0).all() and (alias == np.arange(16)).all()
+
+
+def test_oracle_expectation_sign_tables():
+    # crates/aleph-sv/src/backend.rs:686-714: |0> -> <Z>=1, |1> -> -1, |+> -> <X>=1
+    z0 = np.array([1, 0], dtype=np.complex128)
+    z1 = np.array([0, 1], dtype=np.complex128)
+    plus = np.array([1, 1], dtype=np.complex128) / math.sqrt(2)
+    plus_i = np.array([1, 1j], dtype=np.complex128) / math.sqrt(2)
+    assert oracle.expectation(z0, [(0, "Z")]) == 1.0
+    assert oracle.expectation(z1, [(0, "Z")]) == -1.0
+    assert abs(oracle.expectation(plus, [(0, "X")]) - 1.0) < 1e-15
+    assert abs(oracle.expectation(plus_i, [(0, "Y")]) - 1.0) < 1e-15
+    assert oracle.expectation(z0, [], 2.5) == 2.5
+
+
+def test_oracle_matches_numpy_dense_reference():
+    """Independent check of the oracle's operand order with numpy kron products."""
+    rng = np.random.default_rng(3)
+    n = 5
+    c = C.Circuit(n)
+    mats = []
+    for _ in range(15):
+        qs = [int(x) for x in rng.permutation(n)[:2]]
+        z = rng.standard_normal((4, 4)) + 1j * rng.standard_normal((4, 4))
+        q, _ = np.linalg.qr(z)
+        c.add(C.Unitary2q(q), qs)
+        mats.append((q, qs))
+    psi, _ = oracle.run(n, c.instructions)
+    ref = np.zeros(1 << n, dtype=np.complex128)
+    ref[0] = 1
+    for m, (a, b) in mats:
+        t = ref.reshape([2] * n)  # axis k <-> qubit n-1-k
+        t = np.moveaxis(t, [n - 1 - a, n - 1 - b], [0, 1])
+        sh = t.shape
+        t = (m @ t.reshape(4, -1)).reshape(sh)
+        ref = np.moveaxis(t, [0, 1], [n - 1 - a, n - 1 - b]).reshape(-1)
+    assert np.abs(psi - ref).max() < 1e-13
+
+
+def test_oracle_errors():
+    with pytest.raises(oracle.OracleError) as e:
+        oracle.run(2, [C.GateInstance(C.H(), [2])])
+    assert e.value.status == abi.QUBIT_OUT_OF_RANGE
+    with pytest.raises(oracle.OracleError) as e:
+        oracle.run(2, [C.GateInstance(C.Unitary1q([[1, 1], [0, 1]]), [0])])
+    assert e.value.status == abi.NON_UNITARY_MATRIX
+    with pytest.raises(oracle.OracleError) as e:
+        oracle.run(2, [C.Reset(0)])
+    assert e.value.status == abi.UNSUPPORTED_INSTRUCTION

@@ -1,0 +1,297 @@
+"""GPU parity of the engine against the CPU oracle, through the C ABI.
+
+Tolerances: the plain FP64 path must match the FP64 oracle to
+max |dpsi| <= 1e-12; FP32 to 1e-5 (the reference's FP32 oracle tolerance,
+crates/aleph-oracle/src/harness.rs:27); golden fixtures at 1e-10
+(harness.rs:18). Sampling: given the same variates, bitstrings identical.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from aleph_b200 import circuit as C
+from aleph_b200 import workloads
+from aleph_b200.backend import B200SvBackend, run, run_with_outcomes
+from oracle import oracle
+from tests.fixtures_util import fixture_instructions, fixture_state, load_reference_fixtures
+
+pytestmark = pytest.mark.gpu
+
+F64_TOL = 1e-12
+F32_TOL = 1e-5
+FIXTURES = load_reference_fixtures()
+
+
+def engine_state(circ, precision="f64", uniforms=None, **tuning):
+    be = B200SvBackend(seed=0, precision=precision)
+    for k, v in tuning.items():
+        be.set_tuning(k, v)
+    st, rec = run_with_outcomes(be, circ, uniforms)
+    return be.statevector(st), rec, be, st
+
+
+@pytest.mark.parametrize("fx", FIXTURES, ids=[f["name"] for f in FIXTURES])
+def test_reference_fixtures(fx):
+    c = C.Circuit(fx["num_qubits"], fixture_instructions(fx))
+    got, _, _, _ = engine_state(c, uniforms=fx["measure_uniforms"])
+    want = fixture_state(fx)
+    assert np.abs(got - want).max() <= 1e-10
+    ref, _ = oracle.run(fx["num_qubits"], c.instructions, uniforms=fx["measure_uniforms"])
+    assert np.abs(got - ref).max() <= F64_TOL
+
+
+def random_circuit(n, depth, seed):
+    """Every gate variant, with and without generic controls."""
+    rng = np.random.default_rng(seed)
+    c = C.Circuit(n)
+    one = ["H", "X", "Y", "Z", "S", "Sdg", "T", "Tdg"]
+    par1 = ["Rx", "Ry", "Rz", "Phase"]
+    two = ["Cnot", "Cz", "Swap", "Iswap", "IswapDg"]
+    par2 = ["CRx", "CRy", "CRz"]
+    for _ in range(depth):
+        kind = rng.integers(0, 10)
+        qs = [int(x) for x in rng.permutation(n)[:5]]
+        ctrl = [qs[4]] if rng.random() < 0.25 and n > 4 else []
+        if kind == 0:
+            c.add(C.Gate(str(rng.choice(one))), [qs[0]], ctrl)
+        elif kind == 1:
+            c.add(C.Gate(str(rng.choice(par1)), (float(rng.uniform(-7, 7)),)), [qs[0]], ctrl)
+        elif kind == 2:
+            c.add(C.U3(*rng.uniform(-4, 4, 3)), [qs[0]], ctrl)
+        elif kind == 3:
+            c.add(C.Gate(str(rng.choice(two))), qs[:2], ctrl)
+        elif kind == 4:
+            c.add(C.Gate(str(rng.choice(par2)), (float(rng.uniform(-7, 7)),)), qs[:2], ctrl)
+        elif kind == 5:
+            c.add(C.Gate(str(rng.choice(["Toffoli", "Ccz"]))), qs[:3], ctrl)
+        elif kind == 6:
+            c.add(C.Unitary1q(workloads.haar_su2(rng)), [qs[0]], ctrl)
+        elif kind == 7:
+            z = rng.standard_normal((4, 4)) + 1j * rng.standard_normal((4, 4))
+            q, _ = np.linalg.qr(z)
+            c.add(C.Unitary2q(q), qs[:2], ctrl)
+        elif kind == 8:
+            k = int(rng.integers(2, 6))
+            z = rng.standard_normal((2**k, 2**k)) + 1j * rng.standard_normal((2**k, 2**k))
+            q, _ = np.linalg.qr(z)
+            c.add(C.UnitaryKq(q), qs[:k])
+        else:
+            ph = np.exp(1j * rng.uniform(0, 6.3, 4))
+            if rng.random() < 0.5:
+                c.add(C.Unitary1qDiag(ph[:2]), [qs[0]], ctrl)
+            else:
+                c.add(C.Unitary2qDiag(ph), qs[:2], ctrl)
+    return c
+
+
+@pytest.mark.parametrize("n,smem", [(6, 12), (9, 12), (12, 12), (7, 0), (11, 0), (13, 12), (16, 12), (18, 12)])
+@pytest.mark.parametrize("tile_r", [1, 3, 4, 5])
+def test_random_all_gates_f64(n, smem, tile_r):
+    if n - 5 < 1:
+        pytest.skip("tile path needs n >= 6")
+    c = random_circuit(n, 120, seed=n * 31 + tile_r)
+    got, _, be, _ = engine_state(c, tile_r=tile_r, smem_max_n=smem)
+    want, _ = oracle.run(n, c.instructions)
+    assert np.abs(got - want).max() <= F64_TOL
+
+
+@pytest.mark.parametrize("n", [8, 14, 20])
+def test_brickwall_f64(n):
+    c = workloads.brickwall(n, 20, seed=1)
+    got, _, be, _ = engine_state(c)
+    want, _ = oracle.run(n, c.instructions)
+    assert np.abs(got - want).max() <= F64_TOL
+
+
+@pytest.mark.parametrize("n", [10, 17])
+def test_brickwall_f32(n):
+    c = workloads.brickwall(n, 12, seed=2)
+    got, _, _, _ = engine_state(c, precision="f32")
+    want, _ = oracle.run(n, c.instructions)
+    assert np.abs(got - want).max() <= F32_TOL
+
+
+@pytest.mark.parametrize("n", [9, 16])
+def test_qft_and_qaoa_f64(n):
+    c = workloads.qft_product(n, seed=3)
+    got, _, _, _ = engine_state(c)
+    want, _ = oracle.run(n, c.instructions)
+    assert np.abs(got - want).max() <= F64_TOL
+    rng = np.random.default_rng(4)
+    edges = workloads.random_3_regular(n + (n % 2), rng)
+    m = n + (n % 2)
+    q = workloads.qaoa_maxcut(m, edges, rng.uniform(0, math.pi, 4), rng.uniform(0, math.pi, 4))
+    got, _, _, _ = engine_state(q)
+    want, _ = oracle.run(m, q.instructions)
+    assert np.abs(got - want).max() <= F64_TOL
+
+
+def test_diagonal_phase_instruction():
+    n = 14
+    rng = np.random.default_rng(5)
+    terms = [C.PhaseTerm(tuple(int(x) for x in rng.integers(1, 1 << n, size=int(rng.integers(0, 3)))),
+                         float(rng.uniform(-3, 3))) for _ in range(12)]
+    c = workloads.brickwall(n, 3, seed=6)
+    c.instructions.append(C.DiagonalPhase(n, terms))
+    c.instructions.extend(workloads.brickwall(n, 2, seed=7).instructions)
+    for smem in (0, 12):
+        got, _, _, _ = engine_state(c, smem_max_n=smem)
+        want, _ = oracle.run(n, c.instructions)
+        assert np.abs(got - want).max() <= F64_TOL
+
+
+@pytest.mark.parametrize("n", [6, 14])
+def test_mid_circuit_measurement(n):
+    c = workloads.brickwall(n, 4, seed=8)
+    for q in (0, n - 1, n // 2):
+        c.measure(q, q)
+    c.instructions.extend(workloads.brickwall(n, 3, seed=9).instructions)
+    c.measure(1, 1)
+    us = [0.3, 0.8, 0.5, 0.1]
+    got, rec, _, _ = engine_state(c, uniforms=us)
+    want, outs = oracle.run(n, c.instructions, uniforms=us)
+    assert [int(r.outcome) for r in rec] == outs
+    assert np.abs(got - want).max() <= F64_TOL
+
+
+@pytest.mark.parametrize("n", [1, 5, 12, 18])
+def test_sampling_alias_identical(n):
+    c = workloads.brickwall(n, 6, seed=10) if n > 1 else C.Circuit(1).add(C.Ry(1.1), [0])
+    be = B200SvBackend(seed=0)
+    st = run(be, c)
+    psi = be.statevector(st)
+    words = workloads.splitmix64_words(n, 1024)
+    shots = be.sample(st, 1024, variates=words, mode="alias")
+    assert np.array_equal(shots, oracle.sample_alias(psi, words))
+
+
+@pytest.mark.parametrize("n", [1, 6, 12, 16])
+def test_sampling_cumulative_identical(n):
+    c = workloads.brickwall(n, 6, seed=11) if n > 1 else C.Circuit(1).add(C.Ry(0.7), [0])
+    be = B200SvBackend(seed=0)
+    st = run(be, c)
+    psi = be.statevector(st)
+    u = np.random.default_rng(n).random(2048)
+    u[:4] = [0.0, 0.5, 1.0 - 2**-53, 0.25]
+    shots = be.sample(st, u.size, variates=u, mode="cumulative")
+    assert np.array_equal(shots, oracle.sample_cumulative(psi, u))
+
+
+def test_exact_inverse_boundaries():
+    # exact-probability boundary KAT (see test_cpu_host.test_oracle_exact_inverse_boundaries)
+    psi = np.zeros(512, dtype=np.complex128)
+    psi[[1, 255, 256, 511]] = 0.5
+    be = B200SvBackend(seed=0)
+    st = be.allocate(9)
+    be.set_statevector(st, psi)
+    u = [0.0, np.nextafter(0.25, 0), 0.25, np.nextafter(0.5, 0), 0.5, 0.75, np.nextafter(1.0, 0)]
+    assert list(be.sample(st, len(u), variates=u, mode="cumulative")) == [1, 1, 255, 255, 256, 511, 511]
+    # irrational amplitudes: identical to the oracle whatever the rounding
+    psi2 = np.zeros(512, dtype=np.complex128)
+    for i, p in [(1, 0.125), (255, 0.125), (256, 0.25), (511, 0.5)]:
+        psi2[i] = math.sqrt(p)
+    be.set_statevector(st, psi2)
+    u2 = [0.0, 0.125, np.nextafter(0.25, 0), 0.25, 0.5, np.nextafter(1.0, 0)]
+    assert list(be.sample(st, 6, variates=u2, mode="cumulative")) == list(oracle.sample_cumulative(psi2, u2))
+
+
+def test_alias_table_uniform_and_forced():
+    # uniform superposition: every scaled probability is exactly 1 -> all self-aliased
+    be = B200SvBackend(seed=0)
+    n = 10
+    c = C.Circuit(n)
+    for q in range(n):
+        c.add(C.H(), [q])
+    st = run(be, c)
+    psi = be.statevector(st)
+    words = workloads.splitmix64_words(99, 4096)
+    assert np.array_equal(be.sample(st, 4096, variates=words, mode="alias"), oracle.sample_alias(psi, words))
+    # forced basis state
+    st2 = run(be, C.Circuit(3).add(C.X(), [1]))
+    assert set(be.sample(st2, 64, variates=words[:64], mode="alias").tolist()) == {2}
+
+
+@pytest.mark.parametrize("n", [4, 13])
+def test_expectation_and_probabilities(n):
+    c = workloads.brickwall(n, 5, seed=12)
+    be = B200SvBackend(seed=0)
+    st = run(be, c)
+    psi = be.statevector(st)
+    rng = np.random.default_rng(13)
+    for _ in range(12):
+        k = int(rng.integers(0, min(n, 5) + 1))
+        qs = [int(x) for x in rng.permutation(n)[:k]]
+        ps = [str(x) for x in rng.choice(list("IXYZ"), size=k)]
+        terms = list(zip(qs, ps))
+        coef = float(rng.uniform(-2, 2))
+        assert abs(be.expectation_value(st, terms, coef) - oracle.expectation(psi, terms, coef)) <= 1e-12
+        sub = [int(x) for x in rng.permutation(n)[: int(rng.integers(0, n + 1))]]
+        assert np.abs(be.probabilities(st, sub) - oracle.probabilities(psi, sub)).max() <= 1e-12
+
+
+def test_norm_and_unpermute():
+    n = 13
+    c = workloads.brickwall(n, 4, seed=14)
+    be = B200SvBackend(seed=0)
+    st = run(be, c)
+    psi = be.statevector(st)
+    assert abs(be.norm_sqr(st) - 1.0) <= 1e-12
+    perm = [int(x) for x in np.random.default_rng(15).permutation(n)]
+    be.unpermute_state(st, perm)
+    assert np.abs(be.statevector(st) - oracle.unpermute(psi, perm)).max() == 0.0
+
+
+def test_error_variants():
+    from aleph_b200 import backend as B
+
+    be = B200SvBackend(seed=0)
+    st = be.allocate(3)
+    with pytest.raises(B.QubitOutOfRange):
+        be.apply_gate(st, C.GateInstance(C.H(), [3]))
+    with pytest.raises(B.DuplicateQubit):
+        be.apply_gate(st, C.GateInstance(C.Cnot(), [1, 1]))
+    with pytest.raises(B.DuplicateQubit):
+        be.apply_gate(st, C.GateInstance(C.X(), [1], [1]))
+    with pytest.raises(B.ArityMismatch):
+        be.apply_gate(st, C.GateInstance(C.Cnot(), [0]))
+    with pytest.raises(B.NonFiniteParam):
+        be.apply_gate(st, C.GateInstance(C.Rx(float("nan")), [0]))
+    with pytest.raises(B.NonUnitaryMatrix):
+        be.apply_gate(st, C.GateInstance(C.Unitary1q([[2, 0], [0, 2]]), [0]))
+    with pytest.raises(B.UnsupportedGate):
+        be.apply_gate(st, C.GateInstance(C.UnitaryKq(np.eye(4)), [0, 1], [2]))
+    with pytest.raises(B.UnsupportedInstruction):
+        be.apply_stream(st, [C.Reset(0)])
+    with pytest.raises(B.TooManyQubits):
+        be.allocate(40)
+    with pytest.raises(B.InvalidPauliString):
+        be.expectation_value(st, [(0, "Z")], float("inf"))
+    # a failing stream leaves the state untouched (validation precedes any launch)
+    before = be.statevector(st)
+    with pytest.raises(B.QubitOutOfRange):
+        be.apply_stream(st, [C.GateInstance(C.H(), [0]), C.GateInstance(C.H(), [7])])
+    assert np.array_equal(before, be.statevector(st))
+    # corrupted state -> InvalidState from every query
+    bad = np.zeros(8, dtype=np.complex128)
+    bad[0] = np.nan
+    be.set_statevector(st, bad)
+    for call in (lambda: be.sample(st, 4, variates=[1, 2, 3, 4], mode="alias"),
+                 lambda: be.probabilities(st, [0]),
+                 lambda: be.expectation_value(st, [(0, "Z")]),
+                 lambda: be.measure(st, 0, 0.5)):
+        with pytest.raises(B.InvalidState):
+            call()
+    # degenerate measurement: the zero vector
+    be.set_statevector(st, np.zeros(8))
+    with pytest.raises((B.DegenerateMeasurement, B.InvalidState)):
+        be.measure(st, 0, 0.5)
+
+
+def test_seeded_determinism():
+    c = workloads.brickwall(10, 4, seed=16)
+    a = B200SvBackend(seed=42)
+    b = B200SvBackend(seed=42)
+    sa, sb = run(a, c), run(b, c)
+    assert np.array_equal(a.sample(sa, 500), b.sample(sb, 500))
+    assert a.measure(sa, 3) == b.measure(sb, 3)
