@@ -432,7 +432,7 @@ static int stream_impl(aleph_b200_handle* h, aleph_b200_state* st, const aleph_b
     }
   }
   Plan P;
-  build_plan(ops, st->n, h->opts, &P);
+  if (int s = build_plan(ops, st->n, h->opts, &P)) return set_error(h, s, "optimization pipeline failed: planner");
   // measurement variates: explicit, or drawn from the handle RNG (only the consumed ones advance it)
   std::vector<double> drawn;
   uint64_t saved[4];
@@ -481,7 +481,7 @@ int aleph_b200_apply_diagonal_phase(aleph_b200_handle* h, aleph_b200_state* st, 
   aleph_b200_error_info e{};
   if (lower_diagonal_phase(terms, n_terms, conds, n_conds, &ops[0], &e)) return report(h, e);
   Plan P;
-  build_plan(ops, st->n, h->opts, &P);
+  if (int s = build_plan(ops, st->n, h->opts, &P)) return set_error(h, s, "optimization pipeline failed: planner");
   return execute(h, st, P, nullptr, 0, nullptr, nullptr);
 }
 

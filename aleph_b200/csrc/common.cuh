@@ -99,7 +99,9 @@ __device__ __forceinline__ V2<Real> apply_diag_op(const Op& op, V2<Real> a, uint
       return ((g & op.mask) == op.mask) ? cmul<Real>(ld_coef<Real>(coef + op.coef), a) : a;
     case OP_DIAG: {
       uint32_t idx = 0;
-      for (int i = 0; i < op.nq; ++i) idx = (idx << 1) | (uint32_t)((g >> op.q[i]) & 1);
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+        if (i < op.nq) idx = (idx << 1) | (uint32_t)((g >> op.q[i]) & 1);
       return cmul<Real>(ld_coef<Real>(coef + op.coef + idx), a);
     }
     case OP_POLY: {

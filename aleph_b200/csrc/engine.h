@@ -32,9 +32,12 @@ struct Op {
   uint8_t nq;      // target count in q[]
   uint8_t a, b;    // tile slots of q[0] / q[1] (tile kernel); see TilePass
   uint8_t q[6];    // global target qubits, MSB-first
-  uint8_t pad[2];
+  uint8_t creg;    // tile kernel: control / mask bits that are register qubits (R-bit mask)
+  uint8_t dsrc;    // tile kernel, OP_DIAG: bit i set -> table bit i comes from register slot q[3+i]
   uint64_t ctrl;   // global control mask: op acts where (x & ctrl) == ctrl
-  uint64_t mask;   // OP_CPHASE / OP_NEG: qubit mask; OP_POLY: first term index
+                   // (tile kernel: only the bits outside the register qubits)
+  uint64_t mask;   // OP_CPHASE / OP_NEG: qubit mask (tile kernel: bits outside the
+                   // register qubits; the register part is in creg); OP_POLY: first term
   uint32_t coef;   // offset into the coefficient pool (complex elements)
   uint32_t aux;    // OP_POLY: term count
 };

@@ -473,7 +473,7 @@ void swap_2q_operands(std::vector<double>& c) {
   c = out;
 }
 
-void plan_segment_tiles(const std::vector<const Lowered*>& seg, uint32_t n, uint32_t R, Plan* P) {
+int plan_segment_tiles(const std::vector<const Lowered*>& seg, uint32_t n, uint32_t R, Plan* P) {
   std::vector<const Lowered*> pending = seg;
   while (!pending.empty()) {
     const Lowered* head = pending.front();
@@ -530,8 +530,35 @@ void plan_segment_tiles(const std::vector<const Lowered*>& seg, uint32_t n, uint
       return 255;
     };
     tp.op_begin = (uint32_t)P->ops.size();
+    // Split a global qubit mask into the bits outside the register qubits and
+    // an R-bit mask over the register slots (tested per element in the kernel).
+    auto split = [&](uint64_t m, uint64_t* rest, uint8_t* creg) {
+      *rest = m;
+      *creg = 0;
+      for (uint32_t j = 0; j < R; ++j)
+        if ((m >> tp.hq[j]) & 1) {
+          *creg |= (uint8_t)(1u << j);
+          *rest &= ~(1ull << tp.hq[j]);
+        }
+    };
     for (const Lowered* L : take) {
       Op op = L->op;
+      if (op.type == OP_NEG || op.type == OP_CPHASE) {
+        split(op.mask, &op.mask, &op.creg);
+        op.ctrl = 0;
+      } else if (op.type != OP_POLY) {
+        split(op.ctrl, &op.ctrl, &op.creg);
+      }
+      if (op.type == OP_DIAG) {
+        op.dsrc = 0;
+        for (int i = 0; i < op.nq; ++i) {
+          const uint8_t s = slot(op.q[i]);
+          if (s >= 5 && s != 255) {
+            op.dsrc |= (uint8_t)(1u << i);
+            op.q[3 + i] = (uint8_t)(s - 5);
+          }
+        }
+      }
       if (op.type == OP_1Q || op.type == OP_X) {
         op.a = slot(op.q[0]);
         append_op(P, *L, op);
@@ -554,6 +581,7 @@ void plan_segment_tiles(const std::vector<const Lowered*>& seg, uint32_t n, uint
       }
     }
     tp.op_count = (uint32_t)P->ops.size() - tp.op_begin;
+    if (take.empty()) return ALEPH_B200_OPTIMIZATION;  // no progress: the head op fits no tile
     Pass ps{};
     ps.kind = PASS_TILE;
     ps.tile = tp;
@@ -562,14 +590,16 @@ void plan_segment_tiles(const std::vector<const Lowered*>& seg, uint32_t n, uint
     P->passes.push_back(ps);
     pending.swap(rest);
   }
+  return ALEPH_B200_OK;
 }
 
 }  // namespace
 
 int build_plan(const std::vector<Lowered>& ops, uint32_t n, const PlanOptions& o, Plan* P) {
   std::vector<const Lowered*> seg;
+  int status = ALEPH_B200_OK;
   auto flush = [&]() {
-    if (seg.empty()) return;
+    if (seg.empty() || status) return;
     if (n <= o.smem_max_n || n < 6) {
       Pass ps{};
       ps.kind = PASS_SMEM;
@@ -581,8 +611,9 @@ int build_plan(const std::vector<Lowered>& ops, uint32_t n, const PlanOptions& o
       ps.gates = (uint32_t)seg.size();
       P->passes.push_back(ps);
     } else {
-      const uint32_t R = std::min<uint32_t>(std::max<uint32_t>(o.tile_r, 1), std::min<uint32_t>(5, n - 5));
-      plan_segment_tiles(seg, n, R, P);
+      // a 2-qubit gate may need two register qubits: R >= 2 unless only one high qubit exists
+      const uint32_t R = std::min<uint32_t>(std::max<uint32_t>(o.tile_r, 2), std::min<uint32_t>(5, n - 5));
+      status = plan_segment_tiles(seg, n, R, P);
     }
     seg.clear();
   };
@@ -600,7 +631,7 @@ int build_plan(const std::vector<Lowered>& ops, uint32_t n, const PlanOptions& o
     }
   }
   flush();
-  return ALEPH_B200_OK;
+  return status;
 }
 
 }  // namespace ab
