@@ -162,7 +162,8 @@ int execute(aleph_b200_handle* h, aleph_b200_state* st, const Plan& P, const dou
   const size_t b_pa = al(P.poly_angle.size() * 8), b_po = al(P.poly_off.size() * 4), b_pc = al(P.poly_cnt.size() * 4),
                b_pd = al(P.poly_conds.size() * 8);
   const size_t b_u = al((size_t)n_uniforms * 8), b_s = al(64), b_o = al(P.n_measures + 1);
-  const size_t total = b_ops + b_coef + b_pa + b_po + b_pc + b_pd + b_u + b_s + b_o;
+  const size_t b_img = al(P.block_images.size());
+  const size_t total = b_img + b_ops + b_coef + b_pa + b_po + b_pc + b_pd + b_u + b_s + b_o;
   if (int r = ensure(h, h->plan_buf, total)) return r;
   std::vector<uint8_t> img(total, 0);
   size_t off = 0;
@@ -172,6 +173,7 @@ int execute(aleph_b200_handle* h, aleph_b200_state* st, const Plan& P, const dou
     off += span;
     return at;
   };
+  const size_t o_img = put(P.block_images.data(), P.block_images.size(), b_img);
   const size_t o_ops = put(P.ops.data(), P.ops.size() * sizeof(Op), b_ops);
   const size_t o_coef = f64 ? put(P.coef.data(), P.coef.size() * 8, b_coef) : put(coef32.data(), coef32.size() * 4, b_coef);
   const size_t o_pa = put(P.poly_angle.data(), P.poly_angle.size() * 8, b_pa);
@@ -230,20 +232,35 @@ int execute(aleph_b200_handle* h, aleph_b200_state* st, const Plan& P, const dou
         h->stats.algorithmic_bytes += 3 * len * bpa;
         break;
       case PASS_BLOCK:
-        e = cudaErrorNotSupported;
+        e = launch_block_pass(st->amps, ps.block, (const uint8_t*)(base + o_img), d.ops, d.coef, d.poly,
+                              (int*)(d.status + 4), h->sm_count, h->stream);
+        h->stats.block_passes++;
+        h->stats.passes++;
+        h->stats.algorithmic_bytes += 2 * len * bpa;
         break;
     }
     if (e != cudaSuccess) return cuda_fail(h, e, "kernel launch");
     h->stats.kernel_launches++;
     h->stats.gates_planned += ps.gates;
   }
-  if (status_out || outcomes_out || P.n_measures) {
+  bool any_block = false;
+  for (const Pass& ps : P.passes) any_block |= ps.kind == PASS_BLOCK;
+  if (any_block) {
+    if (int r = ensure(h, h->reduce, (size_t)nb * 3 * 8 + 256)) return r;
+    double* part = (double*)h->reduce.ptr;
+    CK(launch_renormalize(st->amps, st->precision, st->n, part, nb, part + 3 * (size_t)nb, h->stream), "renormalize");
+    h->stats.kernel_launches += 3;
+    h->stats.algorithmic_bytes += 3 * len * bpa;
+  }
+  if (status_out || outcomes_out || P.n_measures || any_block) {
     std::vector<int32_t> stv(16, 0);
     CK(cudaMemcpyAsync(stv.data(), d.status, 16 * 4, cudaMemcpyDeviceToHost, h->stream), "status readback");
     std::vector<uint8_t> oc(P.n_measures + 1, 0);
     if (P.n_measures)
       CK(cudaMemcpyAsync(oc.data(), d.outcomes, P.n_measures, cudaMemcpyDeviceToHost, h->stream), "outcome readback");
     CK(cudaStreamSynchronize(h->stream), "stream synchronize");
+    if (stv[4] != 0)  // a tensor-core block pass gave up on a bounded wait
+      return set_error(h, ALEPH_B200_DEVICE_FAILURE, "device operation failed: block pass wait expired");
     if (status_out) *status_out = stv;
     if (outcomes_out) {
       oc.resize(P.n_measures);
@@ -259,8 +276,6 @@ int execute(aleph_b200_handle* h, aleph_b200_state* st, const Plan& P, const dou
   return 0;
 }
 
-bool valid_handle(aleph_b200_handle* h) { return h != nullptr; }
-
 }  // namespace
 
 extern "C" {
@@ -274,7 +289,8 @@ int aleph_b200_create(uint64_t seed, int device, int precision, aleph_b200_handl
   h->device = device;
   h->precision = precision;
   h->qubit_cap = precision == ALEPH_B200_F64 ? 33 : 34;
-  h->opts.tile_r = precision == ALEPH_B200_F64 ? 4 : 4;
+  h->opts.tile_r = 5;
+  h->opts.tensor_blocks = precision == ALEPH_B200_TC32;
   uint64_t x = seed;
   for (int i = 0; i < 4; ++i) h->x.rng[i] = splitmix64(x);
   cudaError_t e = cudaSetDevice(device);
@@ -557,7 +573,7 @@ static int check_norm_host(aleph_b200_handle* h, aleph_b200_state* st, double* n
     std::snprintf(e.kind, sizeof(e.kind), "non-finite amplitude norm2");
     return report(h, e);
   }
-  if (!std::isfinite(res[0]) || std::fabs(res[0] - 1.0) > std::sqrt(len) * 1e-10) {
+  if (!std::isfinite(res[0]) || std::fabs(res[0] - 1.0) > norm_tolerance(1ull << st->n, st->precision)) {
     aleph_b200_error_info e{};
     e.status = ALEPH_B200_INVALID_STATE;
     std::snprintf(e.kind, sizeof(e.kind), "state norm2 deviates from 1");
@@ -648,7 +664,7 @@ int aleph_b200_expectation(aleph_b200_handle* h, aleph_b200_state* st, const uin
   CK(cudaStreamSynchronize(h->stream), "stream synchronize");
   // validate_state first (measure.rs:166), then coefficient, then qubits (measure.rs:172-193)
   const double len = (double)(1ull << st->n);
-  if (res[1] > 0.0 || !std::isfinite(res[0]) || std::fabs(res[0] - 1.0) > std::sqrt(len) * 1e-10) {
+  if (res[1] > 0.0 || !std::isfinite(res[0]) || std::fabs(res[0] - 1.0) > norm_tolerance((uint64_t)len, st->precision)) {
     aleph_b200_error_info e{};
     e.status = ALEPH_B200_INVALID_STATE;
     std::snprintf(e.kind, sizeof(e.kind), "state norm2 deviates from 1");

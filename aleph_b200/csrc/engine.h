@@ -154,6 +154,14 @@ struct Handle {
   Scratch status;    // device status words (measure outcomes, error flags)
 };
 
+// Accepted |sum |a|^2 - 1| of a state before readout: the FP64 drift budget
+// sqrt(N) * AMPLITUDE_TOL (crates/aleph-sv/src/measure.rs:23-33), and for FP32
+// states the reference FP32 backend's FP32_NORM_TOL = 1e-4
+// (crates/aleph-sv/src/fp32_measure.rs:20-23).
+inline __host__ __device__ double norm_tolerance(uint64_t len, int precision) {
+  return precision == ALEPH_B200_F64 ? sqrt((double)len) * 1e-10 : 1e-4;
+}
+
 // kernels_*.cu entry points (host wrappers; all launch on `stream`)
 cudaError_t launch_init_zero_state(void* amps, uint32_t n, int precision, cudaStream_t s);
 cudaError_t launch_tile_pass(void* amps, int precision, const TilePass& p, const Op* ops, const void* coef,
@@ -164,6 +172,8 @@ cudaError_t launch_kq_pass(void* amps, int precision, uint32_t n, const Op* op_d
                            const void* coef, cudaStream_t s);
 cudaError_t launch_block_pass(void* amps, const BlockPass& p, const uint8_t* images, const Op* ops,
                               const void* coef, PolyTables poly, int* dev_error, int sm_count, cudaStream_t s);
+cudaError_t launch_renormalize(void* amps, int precision, uint32_t n, double* partials, uint32_t nblocks, double* out2,
+                               cudaStream_t s);
 cudaError_t launch_convert(const void* src, int src_prec, void* dst, int dst_prec, uint64_t count, cudaStream_t s);
 cudaError_t launch_unpermute(const void* src, void* dst, int precision, uint32_t n, const uint32_t* perm_dev,
                              cudaStream_t s);
@@ -186,6 +196,10 @@ size_t sample_scratch_bytes(uint32_t n, int mode, uint32_t shots);
 cudaError_t launch_sample(const void* amps, int precision, uint32_t n, uint32_t shots, int mode, const void* variates_dev,
                           uint64_t* out_dev, void* scratch, size_t scratch_bytes, int32_t* status, int sm_count,
                           cudaStream_t s);
+
+// Split-BF16 hi/lo operand images of a 128x128 real matrix (kernels_block.cu), 64 KiB.
+void build_block_image(const double* W, uint8_t* out);
+constexpr uint32_t kBlockImageBytes = 65536;
 
 // planner (planner.cpp)
 int lower_gate(const aleph_b200_instr& g, uint32_t n, const double* pool, uint64_t pool_len, Lowered* out,

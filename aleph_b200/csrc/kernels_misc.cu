@@ -208,4 +208,29 @@ cudaError_t launch_unpermute(const void* src, void* dst, int precision, uint32_t
   return cudaGetLastError();
 }
 
+// ---- renormalisation (end of a tensor-core gate stream) ----------------------
+// Tensor-core FP32 accumulation drifts the state norm systematically (by
+// ~1e-6 per block pass); one FP64 norm reduction and one rescale pass restore
+// |psi| = 1 without a host round trip.
+template <typename Real>
+__global__ void rescale_kernel(V2<Real>* __restrict__ amps, uint64_t len, const double* __restrict__ norm2) {
+  const double s = norm2[0] > 0.0 ? rsqrt(norm2[0]) : 1.0;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < len; i += (uint64_t)gridDim.x * blockDim.x) {
+    const V2<Real> a = ld_amp<Real>(amps + i);
+    st_amp<Real>(amps + i, mk<Real>((Real)(a.x * s), (Real)(a.y * s)));
+  }
+}
+
+cudaError_t launch_renormalize(void* amps, int precision, uint32_t n, double* partials, uint32_t nblocks, double* out2,
+                               cudaStream_t s) {
+  cudaError_t e = launch_norm(amps, precision, n, partials, nblocks, out2, s);
+  if (e != cudaSuccess) return e;
+  const uint64_t len = 1ull << n;
+  const uint64_t b = (len + 255) / 256;
+  const unsigned blocks = (unsigned)(b > 148ull * 32 ? 148ull * 32 : b);
+  if (precision == ALEPH_B200_F64) rescale_kernel<double><<<blocks, 256, 0, s>>>((double2*)amps, len, out2);
+  else rescale_kernel<float><<<blocks, 256, 0, s>>>((float2*)amps, len, out2);
+  return cudaGetLastError();
+}
+
 }  // namespace ab

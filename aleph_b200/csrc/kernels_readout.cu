@@ -102,13 +102,12 @@ __global__ void __launch_bounds__(RB) branch_kernel(const V2<Real>* __restrict__
 // dec[0] = outcome (0/1), dec[1] = 1/norm scale; dval[0] = reported probability.
 __global__ void measure_decide_kernel(const double* __restrict__ sums, uint32_t qubit, uint64_t len,
                                       const double* __restrict__ uniforms, uint32_t n_uniforms, int32_t* status,
-                                      double* dec, uint8_t* outcome_slot) {
+                                      double* dec, uint8_t* outcome_slot, double tol) {
   if (threadIdx.x != 0) return;
   dec[0] = -1.0;  // "skip collapse" unless a decision is made below
   if (status[0] != 0) return;  // an earlier instruction failed: do nothing further
   const double p0r = sums[0], p1r = sums[1], bad = sums[2];
   const double total = p0r + p1r;
-  const double tol = sqrt((double)len) * 1e-10;
   if (bad > 0.0 || !isfinite(total) || fabs(total - 1.0) > tol) {
     status[0] = ALEPH_B200_INVALID_STATE;
     status[2] = (int32_t)qubit;
@@ -175,7 +174,8 @@ cudaError_t launch_measure_pass(void* amps, int precision, uint32_t n, uint32_t 
   if (precision == ALEPH_B200_F64) branch_kernel<double><<<nblocks, RB, 0, s>>>((const double2*)amps, len, qb, partials);
   else branch_kernel<float><<<nblocks, RB, 0, s>>>((const float2*)amps, len, qb, partials);
   finish_kernel<3><<<1, 32, 0, s>>>(partials, nblocks, sums);
-  measure_decide_kernel<<<1, 32, 0, s>>>(sums, qubit, len, uniforms, n_uniforms, status, dec, outcome_slot);
+  measure_decide_kernel<<<1, 32, 0, s>>>(sums, qubit, len, uniforms, n_uniforms, status, dec, outcome_slot,
+                                         norm_tolerance(len, precision));
   const uint64_t b = (len + 255) / 256;
   const unsigned blocks = (unsigned)(b > 148ull * 32 ? 148ull * 32 : b);
   if (precision == ALEPH_B200_F64) collapse_kernel<double><<<blocks, 256, 0, s>>>((double2*)amps, len, qb, dec);

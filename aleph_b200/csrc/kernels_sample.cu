@@ -193,10 +193,10 @@ __global__ void alias_draw_kernel(AliasScratch s, uint64_t mask, const uint64_t*
 }
 
 // Norm check of validate_state (sampling.rs:36-57): sets status on failure.
-__global__ void check_norm_kernel(const double* norm2, uint64_t len, int32_t* status) {
+__global__ void check_norm_kernel(const double* norm2, double tol, int32_t* status) {
   if (threadIdx.x != 0) return;
   const double total = norm2[0];
-  if (norm2[1] > 0.0 || !isfinite(total) || fabs(total - 1.0) > sqrt((double)len) * 1e-10)
+  if (norm2[1] > 0.0 || !isfinite(total) || fabs(total - 1.0) > tol)
     status[0] = ALEPH_B200_INVALID_STATE;
 }
 
@@ -367,7 +367,7 @@ cudaError_t launch_sample(const void* amps, int precision, uint32_t n, uint32_t 
     if (f64) alias_scale_kernel<double><<<nb, PART_B, 0, st>>>((const double2*)amps, len, s);
     else alias_scale_kernel<float><<<nb, PART_B, 0, st>>>((const float2*)amps, len, s);
     alias_offsets_kernel<<<1, 32, 0, st>>>(s, nb, norm2);
-    check_norm_kernel<<<1, 32, 0, st>>>(norm2, len, status);
+    check_norm_kernel<<<1, 32, 0, st>>>(norm2, norm_tolerance(len, precision), status);
     alias_partition_kernel<<<nb, PART_B, 0, st>>>(len, s);
     alias_chain_kernel<<<1, 32, 0, st>>>(len, s, status);
     alias_drain_kernel<<<(unsigned)sm_count * 4, 256, 0, st>>>(s);
@@ -388,7 +388,7 @@ cudaError_t launch_sample(const void* amps, int precision, uint32_t n, uint32_t 
   if (f64) cum_blocks_kernel<double><<<nb, 256, 0, st>>>((const double2*)amps, len, c);
   else cum_blocks_kernel<float><<<nb, 256, 0, st>>>((const float2*)amps, len, c);
   cum_prefix_kernel<<<1, 32, 0, st>>>(c, nb);
-  check_norm_kernel<<<1, 32, 0, st>>>(c.norm, len, status);
+  check_norm_kernel<<<1, 32, 0, st>>>(c.norm, norm_tolerance(len, precision), status);
   if (shots) {
     if (f64)
       cum_draw_kernel<double><<<(shots + 127) / 128, 128, 0, st>>>((const double2*)amps, len, nb, c,

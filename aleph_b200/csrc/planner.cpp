@@ -593,6 +593,174 @@ int plan_segment_tiles(const std::vector<const Lowered*>& seg, uint32_t n, uint3
   return ALEPH_B200_OK;
 }
 
+// ---- tensor-core dense blocks ------------------------------------------------
+// Apply a lowered op to a vector over the block qubits bq[0..6) (index bit b
+// <-> qubit bq[b]); the op's qubits must all be block qubits, except for the
+// diagonal-polynomial case where only the support matters.
+void apply_local(const Lowered& L, const uint32_t* bq, Cx* s) {
+  auto lbit = [&](uint32_t q) -> uint32_t {
+    for (uint32_t b = 0; b < 6; ++b)
+      if (bq[b] == q) return b;
+    return 63;
+  };
+  auto lmask = [&](uint64_t m) -> uint32_t {
+    uint32_t r = 0;
+    for (uint32_t q = 0; q < 64; ++q)
+      if ((m >> q) & 1) r |= 1u << lbit(q);
+    return r;
+  };
+  auto gidx = [&](uint32_t x) -> uint64_t {
+    uint64_t g = 0;
+    for (uint32_t b = 0; b < 6; ++b)
+      if ((x >> b) & 1) g |= 1ull << bq[b];
+    return g;
+  };
+  const Op& op = L.op;
+  const Cx* c = reinterpret_cast<const Cx*>(L.coef.data());
+  switch (op.type) {
+    case OP_NEG:
+    case OP_CPHASE: {
+      const uint32_t m = lmask(op.mask);
+      const Cx f = op.type == OP_NEG ? Cx{-1, 0} : c[0];
+      for (uint32_t x = 0; x < 64; ++x)
+        if ((x & m) == m) s[x] = mul(f, s[x]);
+      return;
+    }
+    case OP_DIAG: {
+      const uint32_t cm = lmask(op.ctrl);
+      for (uint32_t x = 0; x < 64; ++x) {
+        if ((x & cm) != cm) continue;
+        uint32_t idx = 0;
+        for (int i = 0; i < op.nq; ++i) idx = (idx << 1) | ((x >> lbit(op.q[i])) & 1);
+        s[x] = mul(c[idx], s[x]);
+      }
+      return;
+    }
+    case OP_POLY: {
+      for (uint32_t x = 0; x < 64; ++x) {
+        const uint64_t g = gidx(x);
+        double phi = 0.0;
+        size_t off = 0;
+        for (size_t t = 0; t < L.poly_angle.size(); ++t) {
+          bool all = true;
+          for (uint32_t k = 0; k < L.poly_cnt[t]; ++k)
+            if ((__builtin_popcountll(L.poly_conds[off + k] & g) & 1) == 0) all = false;
+          off += L.poly_cnt[t];
+          if (all) phi += L.poly_angle[t];
+        }
+        s[x] = mul(Cx{std::cos(phi), std::sin(phi)}, s[x]);
+      }
+      return;
+    }
+    default: break;
+  }
+  // dense: k targets MSB-first, controls
+  const int k = op.type == OP_2Q ? 2 : op.type == OP_KQ ? op.nq : 1;
+  const uint32_t dim = 1u << k;
+  const uint32_t cm = lmask(op.ctrl);
+  uint32_t tmask = 0, off[32];
+  for (int i = 0; i < k; ++i) tmask |= 1u << lbit(op.q[i]);
+  for (uint32_t r = 0; r < dim; ++r) {
+    uint32_t o = 0;
+    for (int p = 0; p < k; ++p)
+      if ((r >> p) & 1) o |= 1u << lbit(op.q[k - 1 - p]);
+    off[r] = o;
+  }
+  for (uint32_t base = 0; base < 64; ++base) {
+    if ((base & tmask) || (base & cm) != cm) continue;
+    Cx v[32], w[32];
+    for (uint32_t r = 0; r < dim; ++r) v[r] = s[base | off[r]];
+    for (uint32_t r = 0; r < dim; ++r) {
+      if (op.type == OP_X) {
+        w[r] = v[r ^ 1];
+        continue;
+      }
+      Cx acc{0, 0};
+      for (uint32_t cc = 0; cc < dim; ++cc) acc = add(acc, mul(c[r * dim + cc], v[cc]));
+      w[r] = acc;
+    }
+    for (uint32_t r = 0; r < dim; ++r) s[base | off[r]] = w[r];
+  }
+}
+
+int plan_segment_blocks(const std::vector<const Lowered*>& seg, uint32_t n, uint32_t R, Plan* P) {
+  std::vector<const Lowered*> pending = seg;
+  while (!pending.empty()) {
+    uint64_t B = 0, bf = 0, bd = 0, post_lock = 0;
+    std::vector<const Lowered*> take, post, rest;
+    for (const Lowered* L : pending) {
+      const uint64_t supp = L->nondiag | L->diag;
+      if (L->nondiag) {
+        const bool ok = !(L->nondiag & (bf | bd | post_lock)) && !(L->diag & bf) &&
+                        __builtin_popcountll(B | supp) <= 6;
+        if (ok) {
+          B |= supp;
+          take.push_back(L);
+          continue;
+        }
+      } else if (!(L->diag & bf)) {
+        if (__builtin_popcountll(B | supp) <= 6) {
+          B |= supp;
+          take.push_back(L);
+          continue;
+        }
+        if (B != 0) {
+          post.push_back(L);
+          post_lock |= supp;
+          continue;
+        }
+      }
+      bf |= L->nondiag;
+      bd |= L->diag;
+      rest.push_back(L);
+    }
+    if (take.empty()) {
+      // the head op does not fit a 6-qubit block: run it on the CUDA cores
+      std::vector<const Lowered*> one{pending.front()};
+      if (int s = plan_segment_tiles(one, n, R, P)) return s;
+      pending.erase(pending.begin());
+      continue;
+    }
+    // pad the block to 6 qubits with the lowest unused qubits
+    for (uint32_t q = 0; q < n && __builtin_popcountll(B) < 6; ++q) B |= 1ull << q;
+    uint32_t bq[6], nb = 0;
+    for (uint32_t q = 0; q < n; ++q)
+      if ((B >> q) & 1) bq[nb++] = q;
+    // fused unitary, columns = images of the basis vectors
+    std::vector<Cx> U(64 * 64);
+    for (uint32_t col = 0; col < 64; ++col) {
+      Cx s[64];
+      for (uint32_t x = 0; x < 64; ++x) s[x] = Cx{x == col ? 1.0 : 0.0, 0.0};
+      for (const Lowered* L : take) apply_local(*L, bq, s);
+      for (uint32_t x = 0; x < 64; ++x) U[x * 64 + col] = s[x];
+    }
+    std::vector<double> W(128 * 128);
+    for (uint32_t r = 0; r < 64; ++r)
+      for (uint32_t k = 0; k < 64; ++k) {
+        const Cx u = U[r * 64 + k];
+        W[r * 128 + k] = u.re;
+        W[r * 128 + 64 + k] = -u.im;
+        W[(64 + r) * 128 + k] = u.im;
+        W[(64 + r) * 128 + 64 + k] = u.re;
+      }
+    Pass ps{};
+    ps.kind = PASS_BLOCK;
+    ps.block.n = n;
+    for (int j = 0; j < 6; ++j) ps.block.bq[j] = bq[j];
+    ps.block.mat = (uint32_t)P->block_images.size();
+    P->block_images.resize(P->block_images.size() + kBlockImageBytes);
+    build_block_image(W.data(), P->block_images.data() + ps.block.mat);
+    ps.block.post_begin = (uint32_t)P->ops.size();
+    for (const Lowered* L : post) append_op(P, *L, L->op);
+    ps.block.post_count = (uint32_t)P->ops.size() - ps.block.post_begin;
+    ps.record = take.front()->record;
+    ps.gates = (uint32_t)(take.size() + post.size());
+    P->passes.push_back(ps);
+    pending.swap(rest);
+  }
+  return ALEPH_B200_OK;
+}
+
 }  // namespace
 
 int build_plan(const std::vector<Lowered>& ops, uint32_t n, const PlanOptions& o, Plan* P) {
@@ -613,7 +781,8 @@ int build_plan(const std::vector<Lowered>& ops, uint32_t n, const PlanOptions& o
     } else {
       // a 2-qubit gate may need two register qubits: R >= 2 unless only one high qubit exists
       const uint32_t R = std::min<uint32_t>(std::max<uint32_t>(o.tile_r, 2), std::min<uint32_t>(5, n - 5));
-      status = plan_segment_tiles(seg, n, R, P);
+      if (o.tensor_blocks && n >= 13) status = plan_segment_blocks(seg, n, R, P);
+      else status = plan_segment_tiles(seg, n, R, P);
     }
     seg.clear();
   };

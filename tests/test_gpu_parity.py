@@ -295,3 +295,48 @@ def test_seeded_determinism():
     sa, sb = run(a, c), run(b, c)
     assert np.array_equal(a.sample(sa, 500), b.sample(sb, 500))
     assert a.measure(sa, 3) == b.measure(sb, 3)
+
+
+# ---- TC32: fused 6-qubit blocks on tcgen05 tensor cores, split-BF16x3 ---------
+TC_TOL = 1e-5  # per-amplitude, the FP32 tolerance; 1 - fidelity checked at 1e-6
+
+
+def fidelity(a, b):
+    return abs(np.vdot(a, b)) ** 2 / (np.vdot(a, a).real * np.vdot(b, b).real)
+
+
+@pytest.mark.parametrize("n", [13, 14, 18])
+def test_tc32_brickwall(n):
+    c = workloads.brickwall(n, 16, seed=21)
+    got, _, be, _ = engine_state(c, precision="tc32")
+    want, _ = oracle.run(n, c.instructions)
+    assert be.stats()["block_passes"] > 0
+    assert np.abs(got - want).max() <= TC_TOL
+    assert 1.0 - fidelity(got, want) <= 1e-6
+
+
+@pytest.mark.parametrize("n", [13, 16])
+def test_tc32_all_gates(n):
+    c = random_circuit(n, 150, seed=200 + n)
+    got, _, be, _ = engine_state(c, precision="tc32")
+    want, _ = oracle.run(n, c.instructions)
+    assert np.abs(got - want).max() <= TC_TOL
+    assert 1.0 - fidelity(got, want) <= 1e-6
+
+
+def test_tc32_qft_measure_sample():
+    n = 15
+    c = workloads.qft_product(n, seed=22)
+    c.measure(3, 0)
+    c.instructions.extend(workloads.brickwall(n, 3, seed=23).instructions)
+    got, rec, be, st = engine_state(c, precision="tc32", uniforms=[0.4])
+    want, outs = oracle.run(n, c.instructions, uniforms=[0.4])
+    assert [int(r.outcome) for r in rec] == outs
+    assert np.abs(got - want).max() <= TC_TOL
+    # sampling from the FP32 state reads the same probabilities the oracle gets from it
+    psi = be.statevector(st)
+    psi = psi / np.linalg.norm(psi)
+    be.set_statevector(st, psi)
+    words = workloads.splitmix64_words(5, 512)
+    assert np.array_equal(be.sample(st, 512, variates=words, mode="alias"),
+                          oracle.sample_alias(be.statevector(st), words))
