@@ -210,6 +210,13 @@ __global__ void __launch_bounds__(blk::THREADS, 1) block_kernel(const BlockArgs 
   const uint32_t bar_mma = bar_w + 8;
   __shared__ uint32_t tmem_base_sh;
   __shared__ int abort_sh;
+  __shared__ uint64_t tile_base_sh;
+  // post-block diagonal ops: sign flips (CZ-like) as (row mask over j, column-side mask) pairs;
+  // everything else as cached Op records applied per element
+  constexpr int MAX_POST = 48;
+  __shared__ uint64_t neg_rows[MAX_POST], neg_cmask[MAX_POST];
+  __shared__ Op other_ops[MAX_POST];
+  __shared__ int n_neg_sh, n_other_sh;
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const uint32_t n = a.n;
@@ -272,6 +279,27 @@ __global__ void __launch_bounds__(blk::THREADS, 1) block_kernel(const BlockArgs 
     mbar_init(bar_mma, 1);
     fence_barrier_init();
     abort_sh = 0;
+    int nn = 0, no = 0;
+    const uint32_t cnt = a.post_count < (uint32_t)MAX_POST ? a.post_count : (uint32_t)MAX_POST;
+    for (uint32_t o = 0; o < cnt; ++o) {
+      const Op op = a.post[o];
+      if (op.type == OP_NEG) {
+        uint64_t rows = 0;
+        for (int j = 0; j < 64; ++j) {
+          uint64_t gr = 0;
+          for (int b = 0; b < 6; ++b)
+            if ((j >> b) & 1) gr |= 1ull << a.bq[b];
+          if ((gr & op.mask & bmask) == (op.mask & bmask)) rows |= 1ull << j;
+        }
+        neg_rows[nn] = rows;
+        neg_cmask[nn] = op.mask & ~bmask;
+        ++nn;
+      } else {
+        other_ops[no++] = op;
+      }
+    }
+    n_neg_sh = nn;
+    n_other_sh = no;
   }
   if (warp == 0) {
     tmem_alloc(smem_u32(&tmem_base_sh), TMEM_COLS);
@@ -315,7 +343,10 @@ __global__ void __launch_bounds__(blk::THREADS, 1) block_kernel(const BlockArgs 
   uint32_t it = 0;
   for (uint64_t t = first; t < ntiles && !abort_sh; t += stride, ++it) {
     if (!mbar_wait(bar_full, it & 1)) abort_sh = 1;
-    if (tid == 0) bulk_wait_read0();  // the previous tile's store has read the operand buffer
+    if (tid == 0) {
+      bulk_wait_read0();  // the previous tile's store has read the operand buffer
+      tile_base_sh = tile_base(t);
+    }
     __syncthreads();
     if (abort_sh) break;
 
@@ -378,25 +409,29 @@ __global__ void __launch_bounds__(blk::THREADS, 1) block_kernel(const BlockArgs 
       tmem_ld32(tl + 64 + 32 * h, im);
       tc_wait_ld();
       const uint32_t lc = Lcol[col];
-      if (a.post_count) {
-        const uint64_t gc = tile_base(t) | Gcol[col];
-#pragma unroll 4
-        for (int jj = 0; jj < 32; ++jj) {
-          float2 y = make_float2(re[jj], im[jj]);
-          const uint64_t g = gc | Grow[32 * h + jj];
-          for (uint32_t o = 0; o < a.post_count; ++o) y = apply_diag_op<float>(a.post[o], y, g, a.coef, a.poly);
-          out[Lrow[32 * h + jj] | lc] = y;
-        }
-      } else {
+      const uint64_t gc = tile_base_sh | Gcol[col];
+      // sign flips of the CZ-like post ops for this column, as a mask over rows j
+      uint64_t neg = 0;
+      for (int o = 0; o < n_neg_sh; ++o)
+        if ((gc & neg_cmask[o]) == neg_cmask[o]) neg ^= neg_rows[o];
+      const uint32_t negh = (uint32_t)(neg >> (32 * h));
+      const int n_other = n_other_sh;
 #pragma unroll
-        for (int jj = 0; jj < 32; ++jj) out[Lrow[32 * h + jj] | lc] = make_float2(re[jj], im[jj]);
+      for (int jj = 0; jj < 32; ++jj) {
+        float2 y = make_float2(re[jj], im[jj]);
+        if ((negh >> jj) & 1) y = make_float2(-y.x, -y.y);
+        if (n_other) {
+          const uint64_t g = gc | Grow[32 * h + jj];
+          for (int o = 0; o < n_other; ++o) y = apply_diag_op<float>(other_ops[o], y, g, a.coef, a.poly);
+        }
+        out[Lrow[32 * h + jj] | lc] = y;
       }
     }
     tc_fence_before();
     fence_async_smem();
     __syncthreads();
     if (tid == 0) {
-      const uint64_t base = tile_base(t);
+      const uint64_t base = tile_base_sh;
       for (uint32_t r = 0; r < nruns; ++r) bulk_store(a.amps + (base | runoff[r]), sbase + OFF_X + r * run_bytes, run_bytes);
       bulk_commit();
     }

@@ -704,7 +704,7 @@ int plan_segment_blocks(const std::vector<const Lowered*>& seg, uint32_t n, uint
           take.push_back(L);
           continue;
         }
-        if (B != 0) {
+        if (B != 0 && post.size() < 48) {  // the block kernel caches up to 48 post ops
           post.push_back(L);
           post_lock |= supp;
           continue;
