@@ -322,17 +322,23 @@ __global__ void __launch_bounds__(blk::THREADS, 1) block_kernel(const BlockArgs 
     }
     return base;
   };
-  auto issue_tile = [&](uint64_t t) {  // thread 0 only
+  // The runs of a tile are fetched by the 32 lanes of warp 0 together (lane 0
+  // posts the byte count first) and stored back by the lanes of warp 1, so no
+  // single thread serialises up to 64 bulk copies per direction.
+  auto issue_tile = [&](uint64_t t) {  // all lanes of warp 0
     const uint64_t base = tile_base(t);
-    mbar_expect_tx(bar_full, TILE_BYTES);
-    for (uint32_t r = 0; r < nruns; ++r)
+    if (lane == 0) mbar_expect_tx(bar_full, TILE_BYTES);
+    __syncwarp();
+    for (uint32_t r = lane; r < nruns; r += 32)
       bulk_load(sbase + OFF_S + r * run_bytes, a.amps + (base | runoff[r]), run_bytes, bar_full);
   };
 
   const uint64_t first = blockIdx.x, stride = gridDim.x;
-  if (tid == 0) {
-    mbar_expect_tx(bar_w, W_BYTES);
-    bulk_load(sbase + OFF_W, a.image, W_BYTES, bar_w);
+  if (warp == 0) {
+    if (lane == 0) {
+      mbar_expect_tx(bar_w, W_BYTES);
+      bulk_load(sbase + OFF_W, a.image, W_BYTES, bar_w);
+    }
     if (first < ntiles) issue_tile(first);
   }
   if (!mbar_wait(bar_w, 0)) abort_sh = 1;
@@ -343,10 +349,8 @@ __global__ void __launch_bounds__(blk::THREADS, 1) block_kernel(const BlockArgs 
   uint32_t it = 0;
   for (uint64_t t = first; t < ntiles && !abort_sh; t += stride, ++it) {
     if (!mbar_wait(bar_full, it & 1)) abort_sh = 1;
-    if (tid == 0) {
-      bulk_wait_read0();  // the previous tile's store has read the operand buffer
-      tile_base_sh = tile_base(t);
-    }
+    if (warp == 1) bulk_wait_read0();  // each storing lane: its copies have read the operand buffer
+    if (tid == 0) tile_base_sh = tile_base(t);
     __syncthreads();
     if (abort_sh) break;
 
@@ -380,10 +384,12 @@ __global__ void __launch_bounds__(blk::THREADS, 1) block_kernel(const BlockArgs 
     __syncthreads();
     tc_fence_after();
 
-    if (tid == 0) {
+    if (warp == 0) {
       // the input buffer is free: fetch the next tile while this one computes
       const uint64_t nt = t + stride;
       if (nt < ntiles) issue_tile(nt);
+    }
+    if (tid == 32) {
       // ---- 3 x 8 tensor-core MMAs: D = Xh Wh + Xl Wh + Xh Wl ----
       const uint32_t xa[3] = {sbase + OFF_X, sbase + OFF_X + X_PART, sbase + OFF_X};
       const uint32_t wb[3] = {sbase + OFF_W, sbase + OFF_W, sbase + OFF_W + W_BYTES / 2};
@@ -430,14 +436,15 @@ __global__ void __launch_bounds__(blk::THREADS, 1) block_kernel(const BlockArgs 
     tc_fence_before();
     fence_async_smem();
     __syncthreads();
-    if (tid == 0) {
+    if (warp == 1) {
       const uint64_t base = tile_base_sh;
-      for (uint32_t r = 0; r < nruns; ++r) bulk_store(a.amps + (base | runoff[r]), sbase + OFF_X + r * run_bytes, run_bytes);
+      for (uint32_t r = lane; r < nruns; r += 32)
+        bulk_store(a.amps + (base | runoff[r]), sbase + OFF_X + r * run_bytes, run_bytes);
       bulk_commit();
     }
   }
   // drain: bulk copies must finish with shared memory before exit
-  if (tid == 0) bulk_wait0();
+  if (warp == 1) bulk_wait0();
   if (abort_sh) {
     // a fetch may still be in flight after an expired wait: give it a bounded chance to land
     if (tid == 0) mbar_wait(bar_full, it & 1);
