@@ -13,29 +13,27 @@
 // accumulated in FP32 in TMEM: ~16 significant bits per operand at three BF16
 // MMAs per product.
 //
-// The state columns form the MMA's M dimension (TMEM lanes) and the 128 output
-// rows its N dimension, so in the epilogue each thread owns one column with
-// both the real and imaginary part of each of its outputs: complex results
-// (and the diagonal ops that follow the block) stay in registers and go to
-// shared memory as 8-byte stores across consecutive columns.
-//
-// Per CTA (persistent, one per SM, 8 warps):
-//   * W_hi / W_lo arrive once as prebuilt BF16 images in the UMMA canonical
-//     K-major 128-byte-swizzled layout (cp.async.bulk, 64 KiB, the B operand);
-//   * each tile (64 block rows x 128 columns, 64 KiB FP32) is fetched by plain
-//     (non-multicast) cp.async.bulk copies of its contiguous runs, completion
-//     tracked by an mbarrier transaction count; the next tile's fetch is issued
-//     as soon as the current one has been split, overlapping the MMAs, the
-//     epilogue and the store;
-//   * all threads split the tile into X_hi / X_lo (the A operand, same
-//     canonical layout), one thread issues 3 x 8 tcgen05.mma (M=128, N=128,
-//     K=16, kind::f16, BF16 inputs, FP32 accumulate) and commits to an
-//     mbarrier;
-//   * the epilogue reads the accumulator with tcgen05.ld (32x32b), applies
-//     the diagonal ops after the block, writes the FP32 tile into the operand
-//     buffer (free once the MMAs completed) and stores it with cp.async.bulk.
-// Every wait is bounded; on expiry the CTA records an error code, drains its
-// own bulk copies, frees its TMEM and returns.
+// Warp-specialised persistent kernel, one CTA per SM, 10 warps:
+//   * warp 8 (TMA): fetches each tile (64 block rows x 128 columns = 64 KiB
+//     FP32) with plain (non-multicast) cp.async.bulk copies of its contiguous
+//     runs into one of two shared-memory stages (mbarrier transaction counts);
+//   * warps 0-3 (converters): thread c takes column c of the staged tile,
+//     splits its 128 real values into BF16 hi/lo and writes them with
+//     tcgen05.st into TMEM lane c — the A operand of the MMA lives in tensor
+//     memory (two buffers), so shared memory only holds W and the stages;
+//   * warp 9 (one thread): issues 3 x 8 tcgen05.mma (A from TMEM, M=128
+//     columns; B = W_hi / W_lo from shared memory, N=128, K=16; kind::f16,
+//     BF16 in, FP32 accumulate) into one of two TMEM accumulators and commits
+//     to mbarriers that free the A buffer and hand the accumulator over;
+//   * warps 4-7 (epilogue): tcgen05.ld the accumulator (32x32b: one column per
+//     thread, real and imaginary parts of all 64 outputs), apply the diagonal
+//     ops that follow the block (CZ-like sign flips as one 64-bit row mask per
+//     thread, other phases per element) and store straight to HBM.
+// TMEM: accumulators D0, D1 at columns 0 / 128, A0, A1 at 256 / 384 (hi in the
+// first 64 columns, lo in the next 64): all 512 columns.
+// Loads of tile t+2, splits of t+1 and MMAs/stores of t overlap. Every wait
+// is bounded; on expiry the CTA records an error code, every role leaves its
+// loop, the TMEM is freed and the kernel returns.
 
 #include <cstdint>
 #include <cstring>
@@ -48,29 +46,35 @@ namespace ab {
 
 namespace blk {
 
-constexpr int THREADS = 256;
+constexpr int CONV_WARP0 = 0;   // warps 0..3
+constexpr int EPI_WARP0 = 4;    // warps 4..7
+constexpr int TMA_WARP = 8;
+constexpr int MMA_WARP = 9;
+constexpr int THREADS = 10 * 32;
 constexpr int NCOL = 128;                     // columns per tile (MMA M)
 constexpr int TILE_AMPS = 64 * NCOL;          // 8192 complex
 constexpr int TILE_BYTES = TILE_AMPS * 8;     // 64 KiB FP32 complex
 constexpr int W_BYTES = 2 * 128 * 128 * 2;    // hi + lo images, 64 KiB
-constexpr int X_PART = NCOL * 128 * 2;        // one BF16 operand part, 32 KiB
-constexpr uint32_t TMEM_COLS = 128;
-constexpr long long SPIN_LIMIT = 1ll << 28;   // bounded mbarrier waits
+constexpr uint32_t TMEM_COLS = 512;
+constexpr uint32_t TM_D = 0, TM_A = 256;      // accumulators / A operands (128 columns each)
+constexpr long long SPIN_LIMIT = 1ll << 26;   // bounded mbarrier waits
+constexpr int MAX_POST = 48;
 
 // shared-memory map (offsets from a 1024-byte aligned base)
 constexpr int OFF_W = 0;                                  // B operand: W_hi | W_lo
-constexpr int OFF_X = OFF_W + W_BYTES;                    // A operand: X_hi | X_lo, then the FP32 output tile
-constexpr int OFF_S = OFF_X + 2 * X_PART;                 // input tile
-constexpr int OFF_TAB = OFF_S + TILE_BYTES;               // index tables
+constexpr int OFF_S = OFF_W + W_BYTES;                    // two FP32 input stages
+constexpr int OFF_TAB = OFF_S + 2 * TILE_BYTES;           // index tables
 constexpr int TAB_BYTES = 64 * 4 + NCOL * 4 + 64 * 8 + 64 * 8 + NCOL * 8;
 constexpr int OFF_BAR = OFF_TAB + TAB_BYTES;              // mbarriers
-constexpr int SMEM_BYTES = OFF_BAR + 64 + 1024;           // + alignment slack
-static_assert(2 * X_PART == TILE_BYTES, "the output tile reuses the operand buffer");
+constexpr int SMEM_BYTES = OFF_BAR + 128 + 1024;          // + alignment slack
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
 __device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count));
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
 __device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
@@ -86,10 +90,12 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// Bounded wait: false on expiry.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
-  for (long long i = 0; i < SPIN_LIMIT; ++i)
+// Bounded wait: false on expiry or when another role has aborted.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag) {
+  for (long long i = 0; i < SPIN_LIMIT; ++i) {
     if (mbar_try_wait(bar, parity)) return true;
+    if ((i & 1023) == 1023 && *abort_flag) return false;
+  }
   return false;
 }
 __device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
@@ -98,17 +104,10 @@ __device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_
       "l"(src), "r"(bytes), "r"(bar)
       : "memory");
 }
-__device__ __forceinline__ void bulk_store(void* dst, uint32_t src, uint32_t bytes) {
-  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(src), "r"(bytes)
-               : "memory");
-}
-__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void bulk_wait_read0() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
-__device__ __forceinline__ void bulk_wait0() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
-__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 __device__ __forceinline__ void fence_barrier_init() {
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
 __device__ __forceinline__ void tmem_alloc(uint32_t dst_smem, uint32_t ncols) {
   asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(dst_smem), "r"(ncols)
@@ -126,13 +125,14 @@ __device__ __forceinline__ void tc_fence_before() {
 __device__ __forceinline__ void tc_fence_after() {
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 }
-__device__ __forceinline__ void tc_mma(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
-                                       uint32_t accumulate) {
+// D (TMEM) (+)= A (TMEM, K-major) x B (shared memory descriptor)
+__device__ __forceinline__ void tc_mma_ts(uint32_t d_tmem, uint32_t a_tmem, uint64_t b_desc, uint32_t idesc,
+                                          uint32_t accumulate) {
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
       "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
-      "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate)
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n\t}" ::"r"(d_tmem),
+      "r"(a_tmem), "l"(b_desc), "r"(idesc), "r"(accumulate)
       : "memory");
 }
 __device__ __forceinline__ void tc_commit(uint32_t bar) {
@@ -140,6 +140,7 @@ __device__ __forceinline__ void tc_commit(uint32_t bar) {
                : "memory");
 }
 __device__ __forceinline__ void tc_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+__device__ __forceinline__ void tc_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 
 // tcgen05.ld 32 lanes x 32 bit, 32 consecutive columns per thread.
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
@@ -155,6 +156,15 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
       : "r"(taddr));
 #pragma unroll
   for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+// tcgen05.st 32 lanes x 32 bit, 16 consecutive columns per thread.
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t (&r)[16]) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], "
+      "{%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16};" ::"r"(taddr),
+      "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]), "r"(r[8]),
+      "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15])
+      : "memory");
 }
 
 // UMMA shared-memory descriptor: K-major, 128-byte swizzle, 8-row groups 1024 B apart.
@@ -200,32 +210,33 @@ __global__ void __launch_bounds__(blk::THREADS, 1) block_kernel(const BlockArgs 
   extern __shared__ uint8_t smem_raw[];
   uint8_t* sm = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   const uint32_t sbase = smem_u32(sm);
-  uint32_t* Lrow = (uint32_t*)(sm + OFF_TAB);  // local index of block row j
-  uint32_t* Lcol = Lrow + 64;                  // local index of column c
+  uint32_t* Lrow = (uint32_t*)(sm + OFF_TAB);  // tile-local index of block row j
+  uint32_t* Lcol = Lrow + 64;                  // tile-local index of column c
   uint64_t* runoff = (uint64_t*)(Lcol + NCOL); // global offset of run r
   uint64_t* Grow = runoff + 64;                // global offset of block row j
   uint64_t* Gcol = Grow + 64;                  // global offset of column c
-  const uint32_t bar_full = sbase + OFF_BAR;
-  const uint32_t bar_w = bar_full + 8;
-  const uint32_t bar_mma = bar_w + 8;
+  const uint32_t bar_w = sbase + OFF_BAR;
+  const uint32_t bar_sfull = bar_w + 8;         // [2] TMA -> converters
+  const uint32_t bar_sempty = bar_sfull + 16;   // [2] converters -> TMA
+  const uint32_t bar_afull = bar_sempty + 16;   // [2] converters -> MMA
+  const uint32_t bar_aempty = bar_afull + 16;   // [2] MMA -> converters
+  const uint32_t bar_dfull = bar_aempty + 16;   // [2] MMA -> epilogue
+  const uint32_t bar_dempty = bar_dfull + 16;   // [2] epilogue -> MMA
   __shared__ uint32_t tmem_base_sh;
   __shared__ int abort_sh;
-  __shared__ uint64_t tile_base_sh;
-  // post-block diagonal ops: sign flips (CZ-like) as (row mask over j, column-side mask) pairs;
-  // everything else as cached Op records applied per element
-  constexpr int MAX_POST = 48;
   __shared__ uint64_t neg_rows[MAX_POST], neg_cmask[MAX_POST];
   __shared__ Op other_ops[MAX_POST];
   __shared__ int n_neg_sh, n_other_sh;
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const uint32_t n = a.n;
+  volatile int* abort_flag = &abort_sh;
 
   // ---- tile geometry -------------------------------------------------------
   // Tile qubit set T = block qubits + the 7 lowest other qubits (the column
   // bits). T contains all qubits 0..c-1 (one contiguous run of 2^c
-  // amplitudes) plus the block qubits above them; local index bits follow T
-  // in ascending order.
+  // amplitudes) plus the block qubits above them; tile-local index bits
+  // follow T in ascending order.
   uint64_t bmask = 0;
   for (int j = 0; j < 6; ++j) bmask |= 1ull << a.bq[j];
   uint32_t cols[7];
@@ -261,8 +272,7 @@ __global__ void __launch_bounds__(blk::THREADS, 1) block_kernel(const BlockArgs 
       }
     Lrow[tid] = lr;
     Grow[tid] = gr;
-    // run r: local bits c..12 -> the T qubits above c-1
-    uint64_t off = 0;
+    uint64_t off = 0;  // run r: local bits c..12 -> the T qubits above c-1
     if ((uint32_t)tid < nruns) {
       uint32_t bit = 0;
       for (uint32_t q = c; q < n; ++q)
@@ -274,9 +284,15 @@ __global__ void __launch_bounds__(blk::THREADS, 1) block_kernel(const BlockArgs 
     runoff[tid] = off;
   }
   if (tid == 0) {
-    mbar_init(bar_full, 1);
     mbar_init(bar_w, 1);
-    mbar_init(bar_mma, 1);
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(bar_sfull + 8 * b, 1);
+      mbar_init(bar_sempty + 8 * b, 4);
+      mbar_init(bar_afull + 8 * b, 4);
+      mbar_init(bar_aempty + 8 * b, 1);
+      mbar_init(bar_dfull + 8 * b, 1);
+      mbar_init(bar_dempty + 8 * b, 4);
+    }
     fence_barrier_init();
     abort_sh = 0;
     int nn = 0, no = 0;
@@ -305,15 +321,13 @@ __global__ void __launch_bounds__(blk::THREADS, 1) block_kernel(const BlockArgs 
     tmem_alloc(smem_u32(&tmem_base_sh), TMEM_COLS);
     tmem_relinquish();
   }
-  fence_async_smem();
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = tmem_base_sh;
 
   const uint64_t ntiles = 1ull << (n - 13);
-  // deposit a tile index into the non-T qubits
-  auto tile_base = [&](uint64_t t) -> uint64_t {
+  auto tile_base = [&](uint64_t t) -> uint64_t {  // deposit a tile index into the non-tile qubits
     uint64_t base = 0;
     for (uint32_t q = 0; t != 0 && q < n; ++q) {
       if ((tmask >> q) & 1) continue;
@@ -322,136 +336,142 @@ __global__ void __launch_bounds__(blk::THREADS, 1) block_kernel(const BlockArgs 
     }
     return base;
   };
-  // The runs of a tile are fetched by the 32 lanes of warp 0 together (lane 0
-  // posts the byte count first) and stored back by the lanes of warp 1, so no
-  // single thread serialises up to 64 bulk copies per direction.
-  auto issue_tile = [&](uint64_t t) {  // all lanes of warp 0
-    const uint64_t base = tile_base(t);
-    if (lane == 0) mbar_expect_tx(bar_full, TILE_BYTES);
-    __syncwarp();
-    for (uint32_t r = lane; r < nruns; r += 32)
-      bulk_load(sbase + OFF_S + r * run_bytes, a.amps + (base | runoff[r]), run_bytes, bar_full);
-  };
-
   const uint64_t first = blockIdx.x, stride = gridDim.x;
-  if (warp == 0) {
+
+  if (warp == TMA_WARP) {
+    // ---------------- TMA: HBM -> shared-memory stages ----------------
     if (lane == 0) {
       mbar_expect_tx(bar_w, W_BYTES);
       bulk_load(sbase + OFF_W, a.image, W_BYTES, bar_w);
     }
-    if (first < ntiles) issue_tile(first);
-  }
-  if (!mbar_wait(bar_w, 0)) abort_sh = 1;
-  __syncthreads();
-
-  const float2* stg = (const float2*)(sm + OFF_S);
-  float2* out = (float2*)(sm + OFF_X);
-  uint32_t it = 0;
-  for (uint64_t t = first; t < ntiles && !abort_sh; t += stride, ++it) {
-    if (!mbar_wait(bar_full, it & 1)) abort_sh = 1;
-    if (warp == 1) bulk_wait_read0();  // each storing lane: its copies have read the operand buffer
-    if (tid == 0) tile_base_sh = tile_base(t);
-    __syncthreads();
-    if (abort_sh) break;
-
-    // ---- split the FP32 tile into BF16 hi/lo operands (A: 128 columns x K=128) ----
-    // item = (column col, 8-row group g): 8 complex -> 4 x 16-byte chunks
-    for (int item = tid; item < NCOL * 8; item += THREADS) {
-      const int col = item & (NCOL - 1), g = item >> 7;
-      const uint32_t lc = Lcol[col];
-      uint32_t rh[4], rl[4], ih[4], il[4];
-#pragma unroll
-      for (int e = 0; e < 8; e += 2) {
-        const float2 x0 = stg[Lrow[8 * g + e] | lc];
-        const float2 x1 = stg[Lrow[8 * g + e + 1] | lc];
-        const uint32_t h0 = bf16_bits(x0.x), h1 = bf16_bits(x1.x);
-        const uint32_t l0 = bf16_bits(x0.x - bf16_val(h0)), l1 = bf16_bits(x1.x - bf16_val(h1));
-        const uint32_t j0 = bf16_bits(x0.y), j1 = bf16_bits(x1.y);
-        const uint32_t m0 = bf16_bits(x0.y - bf16_val(j0)), m1 = bf16_bits(x1.y - bf16_val(j1));
-        rh[e >> 1] = h0 | (h1 << 16);
-        rl[e >> 1] = l0 | (l1 << 16);
-        ih[e >> 1] = j0 | (j1 << 16);
-        il[e >> 1] = m0 | (m1 << 16);
+    uint32_t i = 0;
+    for (uint64_t t = first; t < ntiles; t += stride, ++i) {
+      const uint32_t s = i & 1, ph = (i >> 1) & 1;
+      if (!mbar_wait(bar_sempty + 8 * s, ph ^ 1, abort_flag)) {
+        abort_sh = 1;
+        break;
       }
-      const uint32_t ore = sw128_off(col, 8 * g, NCOL), oim = sw128_off(col, 64 + 8 * g, NCOL);
-      *(uint4*)(sm + OFF_X + ore) = make_uint4(rh[0], rh[1], rh[2], rh[3]);
-      *(uint4*)(sm + OFF_X + X_PART + ore) = make_uint4(rl[0], rl[1], rl[2], rl[3]);
-      *(uint4*)(sm + OFF_X + oim) = make_uint4(ih[0], ih[1], ih[2], ih[3]);
-      *(uint4*)(sm + OFF_X + X_PART + oim) = make_uint4(il[0], il[1], il[2], il[3]);
-    }
-    fence_async_smem();
-    tc_fence_before();
-    __syncthreads();
-    tc_fence_after();
-
-    if (warp == 0) {
-      // the input buffer is free: fetch the next tile while this one computes
-      const uint64_t nt = t + stride;
-      if (nt < ntiles) issue_tile(nt);
-    }
-    if (tid == 32) {
-      // ---- 3 x 8 tensor-core MMAs: D = Xh Wh + Xl Wh + Xh Wl ----
-      const uint32_t xa[3] = {sbase + OFF_X, sbase + OFF_X + X_PART, sbase + OFF_X};
-      const uint32_t wb[3] = {sbase + OFF_W, sbase + OFF_W, sbase + OFF_W + W_BYTES / 2};
-#pragma unroll
-      for (int term = 0; term < 3; ++term)
-#pragma unroll
-        for (int ks = 0; ks < 8; ++ks) {
-          const uint32_t koff = (ks >> 2) * (128 * 128) + (ks & 3) * 32;  // both operands have 128 rows
-          tc_mma(tmem, sw128_desc(xa[term] + koff), sw128_desc(wb[term] + koff), IDESC, (term | ks) ? 1u : 0u);
-        }
-      tc_commit(bar_mma);
-    }
-    if (!mbar_wait(bar_mma, it & 1)) abort_sh = 1;
-    tc_fence_after();
-
-    // ---- epilogue: TMEM -> registers -> post-block diagonal ops -> FP32 tile ----
-    {
-      const int q = warp & 3, h = warp >> 2;  // columns 32q + lane; block rows 32h..32h+31
-      const int col = 32 * q + lane;
-      float re[32], im[32];
-      const uint32_t tl = tmem + ((uint32_t)(32 * q) << 16);
-      tmem_ld32(tl + 32 * h, re);
-      tmem_ld32(tl + 64 + 32 * h, im);
-      tc_wait_ld();
-      const uint32_t lc = Lcol[col];
-      const uint64_t gc = tile_base_sh | Gcol[col];
-      // sign flips of the CZ-like post ops for this column, as a mask over rows j
-      uint64_t neg = 0;
-      for (int o = 0; o < n_neg_sh; ++o)
-        if ((gc & neg_cmask[o]) == neg_cmask[o]) neg ^= neg_rows[o];
-      const uint32_t negh = (uint32_t)(neg >> (32 * h));
-      const int n_other = n_other_sh;
-#pragma unroll
-      for (int jj = 0; jj < 32; ++jj) {
-        float2 y = make_float2(re[jj], im[jj]);
-        if ((negh >> jj) & 1) y = make_float2(-y.x, -y.y);
-        if (n_other) {
-          const uint64_t g = gc | Grow[32 * h + jj];
-          for (int o = 0; o < n_other; ++o) y = apply_diag_op<float>(other_ops[o], y, g, a.coef, a.poly);
-        }
-        out[Lrow[32 * h + jj] | lc] = y;
-      }
-    }
-    tc_fence_before();
-    fence_async_smem();
-    __syncthreads();
-    if (warp == 1) {
-      const uint64_t base = tile_base_sh;
+      const uint64_t base = tile_base(t);
+      if (lane == 0) mbar_expect_tx(bar_sfull + 8 * s, TILE_BYTES);
+      __syncwarp();
+      const uint32_t dst0 = sbase + OFF_S + s * TILE_BYTES;
       for (uint32_t r = lane; r < nruns; r += 32)
-        bulk_store(a.amps + (base | runoff[r]), sbase + OFF_X + r * run_bytes, run_bytes);
-      bulk_commit();
+        bulk_load(dst0 + r * run_bytes, a.amps + (base | runoff[r]), run_bytes, bar_sfull + 8 * s);
+    }
+  } else if (warp < EPI_WARP0) {
+    // ---------------- converters: stage -> BF16 hi/lo -> TMEM A operand ----------------
+    const int q = warp & 3;
+    const int col = 32 * q + lane;
+    const uint32_t lc = Lcol[col];
+    uint32_t i = 0;
+    for (uint64_t t = first; t < ntiles; t += stride, ++i) {
+      const uint32_t s = i & 1, ph = (i >> 1) & 1;
+      if (!mbar_wait(bar_sfull + 8 * s, ph, abort_flag) || !mbar_wait(bar_aempty + 8 * s, ph ^ 1, abort_flag)) {
+        abort_sh = 1;
+        break;
+      }
+      tc_fence_after();
+      const float2* stg = (const float2*)(sm + OFF_S + s * TILE_BYTES);
+      const uint32_t ta = tmem + TM_A + 128 * s + ((uint32_t)(32 * q) << 16);  // this warp's lanes
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {  // block rows 32h .. 32h+31
+        uint32_t hr[16], hi[16], lr[16], li[16];
+#pragma unroll
+        for (int p = 0; p < 16; ++p) {
+          const float2 x0 = stg[Lrow[32 * h + 2 * p] | lc];
+          const float2 x1 = stg[Lrow[32 * h + 2 * p + 1] | lc];
+          const uint32_t a0 = bf16_bits(x0.x), a1 = bf16_bits(x1.x);
+          const uint32_t b0 = bf16_bits(x0.y), b1 = bf16_bits(x1.y);
+          hr[p] = a0 | (a1 << 16);
+          hi[p] = b0 | (b1 << 16);
+          lr[p] = bf16_bits(x0.x - bf16_val(a0)) | (bf16_bits(x1.x - bf16_val(a1)) << 16);
+          li[p] = bf16_bits(x0.y - bf16_val(b0)) | (bf16_bits(x1.y - bf16_val(b1)) << 16);
+        }
+        // A row layout: K = [Re x_0..63 | Im x_0..63], two BF16 per 32-bit column
+        tmem_st16(ta + 16 * h, hr);            // hi, Re part
+        tmem_st16(ta + 32 + 16 * h, hi);       // hi, Im part
+        tmem_st16(ta + 64 + 16 * h, lr);       // lo, Re part
+        tmem_st16(ta + 64 + 32 + 16 * h, li);  // lo, Im part
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(bar_sempty + 8 * s);  // this warp is done reading the stage
+      tc_wait_st();
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(bar_afull + 8 * s);
+    }
+  } else if (warp == MMA_WARP) {
+    // ---------------- MMA issuer ----------------
+    if (lane == 0) {
+      if (!mbar_wait(bar_w, 0, abort_flag)) abort_sh = 1;
+      uint32_t i = 0;
+      for (uint64_t t = first; t < ntiles && !*abort_flag; t += stride, ++i) {
+        const uint32_t b = i & 1, ph = (i >> 1) & 1;
+        if (!mbar_wait(bar_afull + 8 * b, ph, abort_flag) || !mbar_wait(bar_dempty + 8 * b, ph ^ 1, abort_flag)) {
+          abort_sh = 1;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t d = tmem + TM_D + 128 * b;
+        const uint32_t ah = tmem + TM_A + 128 * b, al = ah + 64;
+        const uint32_t at[3] = {ah, al, ah};
+        const uint32_t wb[3] = {sbase + OFF_W, sbase + OFF_W, sbase + OFF_W + W_BYTES / 2};
+#pragma unroll
+        for (int term = 0; term < 3; ++term)
+#pragma unroll
+          for (int ks = 0; ks < 8; ++ks) {
+            const uint32_t koff = (ks >> 2) * (128 * 128) + (ks & 3) * 32;
+            tc_mma_ts(d, at[term] + 8 * ks, sw128_desc(wb[term] + koff), IDESC, (term | ks) ? 1u : 0u);
+          }
+        tc_commit(bar_aempty + 8 * b);  // A buffer free once these MMAs complete
+        tc_commit(bar_dfull + 8 * b);   // accumulator ready
+      }
+    }
+    __syncwarp();
+  } else {
+    // ---------------- epilogue: TMEM -> registers -> HBM ----------------
+    const int q = warp & 3;  // TMEM lane quarter this warp may access
+    const int col = 32 * q + lane;
+    const int n_neg = n_neg_sh, n_other = n_other_sh;
+    uint32_t i = 0;
+    for (uint64_t t = first; t < ntiles; t += stride, ++i) {
+      const uint32_t b = i & 1, ph = (i >> 1) & 1;
+      const uint64_t gc = tile_base(t) | Gcol[col];
+      uint64_t neg = 0;
+      for (int o = 0; o < n_neg; ++o)
+        if ((gc & neg_cmask[o]) == neg_cmask[o]) neg ^= neg_rows[o];
+      if (!mbar_wait(bar_dfull + 8 * b, ph, abort_flag)) {
+        abort_sh = 1;
+        break;
+      }
+      tc_fence_after();
+      const uint32_t tl = tmem + TM_D + 128 * b + ((uint32_t)(32 * q) << 16);
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        float re[32], im[32];
+        tmem_ld32(tl + 32 * h, re);
+        tmem_ld32(tl + 64 + 32 * h, im);
+        tc_wait_ld();
+        const uint32_t negh = (uint32_t)(neg >> (32 * h));
+#pragma unroll
+        for (int jj = 0; jj < 32; ++jj) {
+          float2 y = make_float2(re[jj], im[jj]);
+          if ((negh >> jj) & 1) y = make_float2(-y.x, -y.y);
+          const uint64_t g = gc | Grow[32 * h + jj];
+          if (n_other)
+            for (int o = 0; o < n_other; ++o) y = apply_diag_op<float>(other_ops[o], y, g, a.coef, a.poly);
+          __stcs(a.amps + g, y);
+        }
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(bar_dempty + 8 * b);
     }
   }
-  // drain: bulk copies must finish with shared memory before exit
-  if (warp == 1) bulk_wait0();
-  if (abort_sh) {
-    // a fetch may still be in flight after an expired wait: give it a bounded chance to land
-    if (tid == 0) mbar_wait(bar_full, it & 1);
-    if (tid == 0) atomicExch(a.err, ALEPH_B200_DEVICE_FAILURE);
-  }
+
   tc_fence_before();
   __syncthreads();
+  if (abort_sh && tid == 0) atomicExch(a.err, ALEPH_B200_DEVICE_FAILURE);
   if (warp == 0) tmem_dealloc(tmem, TMEM_COLS);
 }
 
