@@ -127,6 +127,22 @@ class Stats(ct.Structure):
     ]
 
 
+class PassRecord(ct.Structure):
+    _fields_ = [
+        ("kind", ct.c_uint32),
+        ("gates", ct.c_uint32),
+        ("n", ct.c_uint32),
+        ("nq", ct.c_uint32),
+        ("qubits", ct.c_uint32 * 8),
+        ("post_ops", ct.c_uint32),
+        ("pad", ct.c_uint32),
+        ("ms", ct.c_double),
+        ("bytes", ct.c_double),
+    ]
+
+
+PASS_KINDS = {1: "tile", 2: "smem", 3: "kq", 4: "measure", 5: "block", 6: "renorm"}
+
 # Every symbol include/aleph_b200.h declares, with its ctypes signature.
 _P = ct.c_void_p
 _SIGNATURES = {
@@ -157,6 +173,7 @@ _SIGNATURES = {
     "aleph_b200_last_error": ([_P, ct.c_char_p, ct.c_uint64], ct.c_int),
     "aleph_b200_last_error_info": ([_P, ct.POINTER(ErrorInfo)], ct.c_int),
     "aleph_b200_set_tuning": ([_P, ct.c_char_p, ct.c_int64], ct.c_int),
+    "aleph_b200_get_pass_records": ([_P, ct.POINTER(PassRecord), ct.c_uint64, ct.POINTER(ct.c_uint64)], ct.c_int),
     "aleph_b200_get_stats": ([_P, ct.POINTER(Stats)], ct.c_int),
     "aleph_b200_reset_stats": ([_P], ct.c_int),
 }

@@ -217,6 +217,18 @@ class B200SvBackend:
     def reset_stats(self):
         self.lib.aleph_b200_reset_stats(self.handle)
 
+    def pass_records(self) -> list[dict]:
+        """Per-pass device timings of the last stream run with ``record_passes`` on."""
+        n = ct.c_uint64()
+        self.lib.aleph_b200_get_pass_records(self.handle, None, 0, ct.byref(n))
+        buf = (abi.PassRecord * max(1, n.value))()
+        self._check(self.lib.aleph_b200_get_pass_records(self.handle, buf, n.value, ct.byref(n)))
+        out = []
+        for r in buf[: n.value]:
+            out.append({"kind": abi.PASS_KINDS.get(r.kind, r.kind), "gates": r.gates, "n": r.n,
+                        "qubits": list(r.qubits[: r.nq]), "post_ops": r.post_ops, "ms": r.ms, "bytes": r.bytes})
+        return out
+
     def apply_stream(self, state: State, instructions, measure_uniforms=None, flat: Flat | None = None):
         """Apply a whole instruction list in one call; returns measurement outcomes."""
         flat = flat or flatten(instructions)

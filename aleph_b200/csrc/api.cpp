@@ -203,8 +203,37 @@ int execute(aleph_b200_handle* h, aleph_b200_state* st, const Plan& P, const dou
   const double bpa = f64 ? 16.0 : 8.0;
   const double len = (double)(1ull << st->n);
   uint32_t mi = 0;
+  const bool rec = h->record_passes;
+  if (rec) {
+    h->records.clear();
+    const size_t need = 2 * (P.passes.size() + 1);
+    while (h->events.size() < need) {
+      cudaEvent_t ev;
+      CK(cudaEventCreate(&ev), "event create");
+      h->events.push_back(ev);
+    }
+  }
+  auto record_begin = [&](size_t k) -> cudaError_t {
+    return rec ? cudaEventRecord(h->events[2 * k], h->stream) : cudaSuccess;
+  };
+  auto record_end = [&](size_t k, uint32_t kind, uint32_t gates, uint32_t nq, const uint32_t* qs, uint32_t post,
+                        double bytes) -> cudaError_t {
+    if (!rec) return cudaSuccess;
+    aleph_b200_pass_record r{};
+    r.kind = kind;
+    r.gates = gates;
+    r.n = st->n;
+    r.nq = nq;
+    for (uint32_t j = 0; j < nq && j < 8; ++j) r.qubits[j] = qs[j];
+    r.post_ops = post;
+    r.bytes = bytes;
+    h->records.push_back(r);
+    return cudaEventRecord(h->events[2 * k + 1], h->stream);
+  };
+  size_t pk = 0;
   for (const Pass& ps : P.passes) {
-    cudaError_t e = cudaSuccess;
+    cudaError_t e = record_begin(pk);
+    if (e != cudaSuccess) return cuda_fail(h, e, "event record");
     switch (ps.kind) {
       case PASS_TILE:
         e = launch_tile_pass(st->amps, st->precision, ps.tile, d.ops, d.coef, d.poly, h->stream);
@@ -242,15 +271,34 @@ int execute(aleph_b200_handle* h, aleph_b200_state* st, const Plan& P, const dou
     if (e != cudaSuccess) return cuda_fail(h, e, "kernel launch");
     h->stats.kernel_launches++;
     h->stats.gates_planned += ps.gates;
+    {
+      const uint32_t* qs = ps.kind == PASS_BLOCK ? ps.block.bq : ps.tile.hq;
+      const uint32_t nq = ps.kind == PASS_BLOCK ? 6 : ps.kind == PASS_TILE ? ps.tile.R : 0;
+      const double bytes = ps.kind == PASS_MEASURE ? 3 * len * bpa : 2 * len * bpa;
+      CK(record_end(pk, (uint32_t)ps.kind, ps.gates, nq, qs, ps.kind == PASS_BLOCK ? ps.block.post_count : 0, bytes),
+         "event record");
+    }
+    ++pk;
   }
   bool any_block = false;
   for (const Pass& ps : P.passes) any_block |= ps.kind == PASS_BLOCK;
   if (any_block) {
     if (int r = ensure(h, h->reduce, (size_t)nb * 3 * 8 + 256)) return r;
     double* part = (double*)h->reduce.ptr;
+    CK(record_begin(pk), "event record");
     CK(launch_renormalize(st->amps, st->precision, st->n, part, nb, part + 3 * (size_t)nb, h->stream), "renormalize");
+    CK(record_end(pk, 6, 0, 0, nullptr, 0, 3 * len * bpa), "event record");
+    ++pk;
     h->stats.kernel_launches += 3;
     h->stats.algorithmic_bytes += 3 * len * bpa;
+  }
+  if (rec) {
+    CK(cudaStreamSynchronize(h->stream), "stream synchronize");
+    for (size_t k = 0; k < h->records.size(); ++k) {
+      float ms = 0.f;
+      CK(cudaEventElapsedTime(&ms, h->events[2 * k], h->events[2 * k + 1]), "event elapsed");
+      h->records[k].ms = ms;
+    }
   }
   if (status_out || outcomes_out || P.n_measures || any_block) {
     std::vector<int32_t> stv(16, 0);
@@ -310,6 +358,7 @@ int aleph_b200_destroy(aleph_b200_handle* h) {
   if (h->stream) cudaStreamSynchronize(h->stream);
   for (Scratch* s : {&h->reduce, &h->plan_buf, &h->sample, &h->status})
     if (s->ptr) cudaFree(s->ptr);
+  for (cudaEvent_t ev : h->events) cudaEventDestroy(ev);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete static_cast<FullHandle*>(h);
   return ALEPH_B200_OK;
@@ -815,12 +864,23 @@ int aleph_b200_set_tuning(aleph_b200_handle* h, const char* key, int64_t value) 
     h->opts.tile_r = (uint32_t)value;
     return ALEPH_B200_OK;
   }
+  if (!std::strcmp(key, "record_passes")) {
+    h->record_passes = value != 0;
+    return ALEPH_B200_OK;
+  }
   if (!std::strcmp(key, "smem_max_n")) {
     if (value < 0 || value > 12) return set_error(h, ALEPH_B200_INVALID_ARGUMENT, "smem_max_n must be in 0..12");
     h->opts.smem_max_n = (uint32_t)value;
     return ALEPH_B200_OK;
   }
   return set_error(h, ALEPH_B200_INVALID_ARGUMENT, "unknown tuning key %s", key);
+}
+
+int aleph_b200_get_pass_records(const aleph_b200_handle* h, aleph_b200_pass_record* out, uint64_t cap, uint64_t* n) {
+  if (!h || !n || (cap && !out)) return ALEPH_B200_INVALID_ARGUMENT;
+  *n = h->records.size();
+  for (size_t i = 0; i < h->records.size() && i < cap; ++i) out[i] = h->records[i];
+  return ALEPH_B200_OK;
 }
 
 int aleph_b200_get_stats(const aleph_b200_handle* h, aleph_b200_stats* out) {

@@ -152,6 +152,10 @@ struct Handle {
   Scratch plan_buf;  // uploaded plan tables
   Scratch sample;    // sampling tables
   Scratch status;    // device status words (measure outcomes, error flags)
+  // per-pass timing (record_passes)
+  bool record_passes = false;
+  std::vector<cudaEvent_t> events;
+  std::vector<aleph_b200_pass_record> records;
 };
 
 // Accepted |sum |a|^2 - 1| of a state before readout: the FP64 drift budget

@@ -46,11 +46,12 @@ namespace ab {
 
 namespace blk {
 
-constexpr int CONV_WARP0 = 0;   // warps 0..3
-constexpr int EPI_WARP0 = 4;    // warps 4..7
-constexpr int TMA_WARP = 8;
-constexpr int MMA_WARP = 9;
-constexpr int THREADS = 10 * 32;
+constexpr int CONV_WARP0 = 0;   // warps 0..7: two per TMEM lane quarter, one per half of the block rows
+constexpr int EPI_WARP0 = 8;    // warps 8..15: same split
+constexpr int TMA_WARP = 16;
+constexpr int MMA_WARP = 17;
+constexpr int THREADS = 18 * 32;
+constexpr int ROLE_WARPS = 8;   // converter / epilogue warps (mbarrier arrival counts)
 constexpr int NCOL = 128;                     // columns per tile (MMA M)
 constexpr int TILE_AMPS = 64 * NCOL;          // 8192 complex
 constexpr int TILE_BYTES = TILE_AMPS * 8;     // 64 KiB FP32 complex
@@ -203,9 +204,14 @@ struct BlockArgs {
   int* err;
   uint32_t n;
   uint32_t bq[6];
+  // Per block row j: tile-local index and global offset. Kept in the
+  // kernel-parameter (constant) bank so the unrolled per-element loops of the
+  // converters and the epilogue read them as instruction operands.
+  uint32_t lrow[64];
+  uint64_t grow[64];
 };
 
-__global__ void __launch_bounds__(blk::THREADS, 1) block_kernel(const BlockArgs a) {
+__global__ void __launch_bounds__(blk::THREADS, 1) block_kernel(const __grid_constant__ BlockArgs a) {
   using namespace blk;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* sm = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -287,11 +293,11 @@ __global__ void __launch_bounds__(blk::THREADS, 1) block_kernel(const BlockArgs 
     mbar_init(bar_w, 1);
     for (int b = 0; b < 2; ++b) {
       mbar_init(bar_sfull + 8 * b, 1);
-      mbar_init(bar_sempty + 8 * b, 4);
-      mbar_init(bar_afull + 8 * b, 4);
+      mbar_init(bar_sempty + 8 * b, ROLE_WARPS);
+      mbar_init(bar_afull + 8 * b, ROLE_WARPS);
       mbar_init(bar_aempty + 8 * b, 1);
       mbar_init(bar_dfull + 8 * b, 1);
-      mbar_init(bar_dempty + 8 * b, 4);
+      mbar_init(bar_dempty + 8 * b, ROLE_WARPS);
     }
     fence_barrier_init();
     abort_sh = 0;
@@ -360,7 +366,8 @@ __global__ void __launch_bounds__(blk::THREADS, 1) block_kernel(const BlockArgs 
     }
   } else if (warp < EPI_WARP0) {
     // ---------------- converters: stage -> BF16 hi/lo -> TMEM A operand ----------------
-    const int q = warp & 3;
+    const int q = warp & 3;  // TMEM lane quarter
+    const int h = (warp - CONV_WARP0) >> 2;  // block rows 32h .. 32h+31
     const int col = 32 * q + lane;
     const uint32_t lc = Lcol[col];
     uint32_t i = 0;
@@ -373,13 +380,14 @@ __global__ void __launch_bounds__(blk::THREADS, 1) block_kernel(const BlockArgs 
       tc_fence_after();
       const float2* stg = (const float2*)(sm + OFF_S + s * TILE_BYTES);
       const uint32_t ta = tmem + TM_A + 128 * s + ((uint32_t)(32 * q) << 16);  // this warp's lanes
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {  // block rows 32h .. 32h+31
+      {
         uint32_t hr[16], hi[16], lr[16], li[16];
 #pragma unroll
         for (int p = 0; p < 16; ++p) {
-          const float2 x0 = stg[Lrow[32 * h + 2 * p] | lc];
-          const float2 x1 = stg[Lrow[32 * h + 2 * p + 1] | lc];
+          const uint32_t r0 = h ? a.lrow[32 + 2 * p] : a.lrow[2 * p];
+          const uint32_t r1 = h ? a.lrow[33 + 2 * p] : a.lrow[2 * p + 1];
+          const float2 x0 = stg[r0 | lc];
+          const float2 x1 = stg[r1 | lc];
           const uint32_t a0 = bf16_bits(x0.x), a1 = bf16_bits(x1.x);
           const uint32_t b0 = bf16_bits(x0.y), b1 = bf16_bits(x1.y);
           hr[p] = a0 | (a1 << 16);
@@ -431,6 +439,7 @@ __global__ void __launch_bounds__(blk::THREADS, 1) block_kernel(const BlockArgs 
   } else {
     // ---------------- epilogue: TMEM -> registers -> HBM ----------------
     const int q = warp & 3;  // TMEM lane quarter this warp may access
+    const int h = (warp - EPI_WARP0) >> 2;  // block rows 32h .. 32h+31
     const int col = 32 * q + lane;
     const int n_neg = n_neg_sh, n_other = n_other_sh;
     uint32_t i = 0;
@@ -446,21 +455,21 @@ __global__ void __launch_bounds__(blk::THREADS, 1) block_kernel(const BlockArgs 
       }
       tc_fence_after();
       const uint32_t tl = tmem + TM_D + 128 * b + ((uint32_t)(32 * q) << 16);
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
+      {
         float re[32], im[32];
         tmem_ld32(tl + 32 * h, re);
         tmem_ld32(tl + 64 + 32 * h, im);
         tc_wait_ld();
         const uint32_t negh = (uint32_t)(neg >> (32 * h));
+        float2* pc = a.amps + gc;
 #pragma unroll
         for (int jj = 0; jj < 32; ++jj) {
           float2 y = make_float2(re[jj], im[jj]);
           if ((negh >> jj) & 1) y = make_float2(-y.x, -y.y);
-          const uint64_t g = gc | Grow[32 * h + jj];
+          const uint64_t gr = h ? a.grow[32 + jj] : a.grow[jj];
           if (n_other)
-            for (int o = 0; o < n_other; ++o) y = apply_diag_op<float>(other_ops[o], y, g, a.coef, a.poly);
-          __stcs(a.amps + g, y);
+            for (int o = 0; o < n_other; ++o) y = apply_diag_op<float>(other_ops[o], y, gc | gr, a.coef, a.poly);
+          __stcs(pc + gr, y);
         }
       }
       tc_fence_before();
@@ -488,6 +497,28 @@ cudaError_t launch_block_pass(void* amps, const BlockPass& p, const uint8_t* ima
   a.err = dev_error;
   a.n = p.n;
   for (int j = 0; j < 6; ++j) a.bq[j] = p.bq[j];
+  {
+    // tile geometry, as in the kernel: T = block qubits + the 7 lowest other qubits
+    uint64_t bmask = 0;
+    for (int j = 0; j < 6; ++j) bmask |= 1ull << p.bq[j];
+    uint64_t tmask = bmask;
+    for (uint32_t q = 0, k = 0; q < p.n && k < 7; ++q)
+      if (!((bmask >> q) & 1)) {
+        tmask |= 1ull << q;
+        ++k;
+      }
+    for (uint32_t j = 0; j < 64; ++j) {
+      uint32_t lr = 0;
+      uint64_t gr = 0;
+      for (int b = 0; b < 6; ++b)
+        if ((j >> b) & 1) {
+          lr |= 1u << __builtin_popcountll(tmask & ((1ull << p.bq[b]) - 1));
+          gr |= 1ull << p.bq[b];
+        }
+      a.lrow[j] = lr;
+      a.grow[j] = gr;
+    }
+  }
   static bool attr = false;
   if (!attr) {
     cudaError_t e = cudaFuncSetAttribute(block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, blk::SMEM_BYTES);

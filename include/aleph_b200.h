@@ -242,8 +242,26 @@ int aleph_b200_last_error_info(const aleph_b200_handle* h, aleph_b200_error_info
 
 /* ---- planner tuning (the autotuner's knobs) ----
  * keys: "tile_r" (register qubits per warp tile, 1..5), "smem_max_n" (states
- * with n <= this run as one shared-memory pass, 0..12). */
+ * with n <= this run as one shared-memory pass, 0..12), "record_passes"
+ * (0/1: time every pass of later gate streams with CUDA events). */
 int aleph_b200_set_tuning(aleph_b200_handle* h, const char* key, int64_t value);
+
+/* ---- per-pass timing records (training data of the learned fusion planner) ---- */
+typedef struct aleph_b200_pass_record {
+  uint32_t kind;        /* 1 = CUDA-core tile pass, 2 = shared-memory pass, 3 = dense k-qubit,
+                           4 = measurement, 5 = tensor-core dense block, 6 = renormalisation */
+  uint32_t gates;       /* gates the pass applied                                          */
+  uint32_t n;           /* state qubits                                                    */
+  uint32_t nq;          /* entries used in qubits[]                                        */
+  uint32_t qubits[8];   /* tile register qubits / block qubits                             */
+  uint32_t post_ops;    /* diagonal ops after a block                                      */
+  uint32_t pad;
+  double ms;            /* device time of the pass (CUDA events on the handle's stream)    */
+  double bytes;         /* algorithmic HBM bytes of the pass                               */
+} aleph_b200_pass_record;
+/* Records of the last gate stream run with "record_passes" on; *n = count. */
+int aleph_b200_get_pass_records(const aleph_b200_handle* h, aleph_b200_pass_record* out, uint64_t cap,
+                                uint64_t* n);
 
 /* ---- launch statistics (execution_counters, crates/aleph-cuda/src/execution.rs:145-165) ---- */
 typedef struct aleph_b200_stats {
