@@ -124,6 +124,8 @@ class Stats(ct.Structure):
         ("block_passes", ct.c_uint64),
         ("gates_planned", ct.c_uint64),
         ("algorithmic_bytes", ct.c_double),
+        ("h2d_bytes", ct.c_uint64),
+        ("d2h_bytes", ct.c_uint64),
     ]
 
 
@@ -156,6 +158,12 @@ _SIGNATURES = {
     "aleph_b200_apply_gate_stream": (
         [_P, _P, ct.POINTER(Instr), ct.c_uint64, ct.POINTER(Pools), ct.POINTER(ct.c_double), ct.c_uint64,
          ct.POINTER(ct.c_uint8), ct.c_uint64, ct.POINTER(ct.c_uint64)], ct.c_int),
+    "aleph_b200_compile": (
+        [_P, ct.c_uint32, ct.POINTER(Instr), ct.c_uint64, ct.POINTER(Pools), ct.POINTER(_P)], ct.c_int),
+    "aleph_b200_execute": (
+        [_P, _P, _P, ct.POINTER(ct.c_double), ct.c_uint64, ct.POINTER(ct.c_uint8), ct.c_uint64,
+         ct.POINTER(ct.c_uint64)], ct.c_int),
+    "aleph_b200_plan_free": ([_P, _P], ct.c_int),
     "aleph_b200_apply_diagonal_phase": (
         [_P, _P, ct.POINTER(PhaseTerm), ct.c_uint64, ct.POINTER(ct.c_uint64), ct.c_uint64], ct.c_int),
     "aleph_b200_unpermute": ([_P, _P, ct.POINTER(ct.c_uint32), ct.c_uint32], ct.c_int),
@@ -170,6 +178,8 @@ _SIGNATURES = {
     "aleph_b200_set_amplitudes": ([_P, _P, ct.POINTER(ct.c_double)], ct.c_int),
     "aleph_b200_norm_sqr": ([_P, _P, ct.POINTER(ct.c_double)], ct.c_int),
     "aleph_b200_synchronize": ([_P], ct.c_int),
+    "aleph_b200_get_stream": ([_P, ct.POINTER(_P)], ct.c_int),
+    "aleph_b200_reset_state": ([_P, _P], ct.c_int),
     "aleph_b200_last_error": ([_P, ct.c_char_p, ct.c_uint64], ct.c_int),
     "aleph_b200_last_error_info": ([_P, ct.POINTER(ErrorInfo)], ct.c_int),
     "aleph_b200_set_tuning": ([_P, ct.c_char_p, ct.c_int64], ct.c_int),

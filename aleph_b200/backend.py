@@ -206,6 +206,16 @@ class B200SvBackend:
         self._check(self.lib.aleph_b200_norm_sqr(self.handle, state.ptr, ct.byref(out)))
         return out.value
 
+    def reset_state(self, state: State) -> None:
+        """Back to |0...0> on the device, reusing the allocation."""
+        self._check(self.lib.aleph_b200_reset_state(self.handle, state.ptr))
+
+    def stream_ptr(self) -> int:
+        """The handle's cudaStream_t (every engine kernel runs on it)."""
+        p = ct.c_void_p()
+        self._check(self.lib.aleph_b200_get_stream(self.handle, ct.byref(p)))
+        return p.value or 0
+
     def synchronize(self):
         self._check(self.lib.aleph_b200_synchronize(self.handle))
 
@@ -240,6 +250,46 @@ class B200SvBackend:
             u.ctypes.data_as(ct.POINTER(ct.c_double)) if u is not None and u.size else None,
             0 if u is None else u.size, outs, flat.n, ct.byref(nout)))
         return [int(outs[i]) for i in range(nout.value)]
+
+
+    def compile(self, num_qubits: int, instructions) -> "CompiledPlan":
+        """``CudaExecutionPlan::compile`` (crates/aleph-cuda/src/execution.rs:78): validate
+        and plan once; the plan tables stay resident on the device."""
+        flat = instructions if isinstance(instructions, Flat) else flatten(instructions)
+        p = ct.c_void_p()
+        self._check(self.lib.aleph_b200_compile(self.handle, num_qubits, flat.instrs, flat.n,
+                                                ct.byref(flat.pools), ct.byref(p)))
+        return CompiledPlan(p, num_qubits, flat, self)
+
+
+class CompiledPlan:
+    """A plan compiled by :meth:`B200SvBackend.compile`; ``execute`` applies it
+    (``CudaExecutionPlan::execute``, crates/aleph-cuda/src/execution.rs:183)."""
+
+    def __init__(self, ptr, num_qubits: int, flat: Flat, backend: B200SvBackend):
+        self.ptr, self.num_qubits, self.flat, self.backend = ptr, num_qubits, flat, backend
+        self._outs = (ct.c_uint8 * max(1, flat.n))()
+
+    def execute(self, state: State, measure_uniforms=None) -> list[int]:
+        b = self.backend
+        u = None if measure_uniforms is None else np.ascontiguousarray(np.asarray(measure_uniforms, np.float64))
+        nout = ct.c_uint64()
+        b._check(b.lib.aleph_b200_execute(
+            b.handle, state.ptr, self.ptr,
+            u.ctypes.data_as(ct.POINTER(ct.c_double)) if u is not None and u.size else None,
+            0 if u is None else u.size, self._outs, self.flat.n, ct.byref(nout)))
+        return [int(self._outs[i]) for i in range(nout.value)]
+
+    def free(self) -> None:
+        if self.ptr:
+            self.backend.lib.aleph_b200_plan_free(self.backend.handle, self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
 
 
 def run_with_outcomes(backend: B200SvBackend, circuit: Circuit, measure_uniforms=None):

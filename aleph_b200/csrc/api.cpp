@@ -130,6 +130,15 @@ int ensure(aleph_b200_handle* h, Scratch& s, size_t bytes) {
   return 0;
 }
 
+// Every host<->device copy of the engine goes through here so that the
+// stats count the bytes that cross PCIe/C2C.
+cudaError_t copy_async(aleph_b200_handle* h, void* dst, const void* src, size_t bytes, cudaMemcpyKind kind,
+                       cudaStream_t s) {
+  if (kind == cudaMemcpyHostToDevice) h->stats.h2d_bytes += bytes;
+  if (kind == cudaMemcpyDeviceToHost) h->stats.d2h_bytes += bytes;
+  return cudaMemcpyAsync(dst, src, bytes, kind, s);
+}
+
 int bind(aleph_b200_handle* h) {
   cudaError_t e = cudaSetDevice(h->device);
   if (e != cudaSuccess) return cuda_fail(h, e, "cudaSetDevice");
@@ -148,34 +157,42 @@ struct DevPlan {
 
 size_t al(size_t x) { return (x + 255) & ~(size_t)255; }
 
+// Runs a plan on a state. With `cache` (a compiled plan's own device buffer),
+// the plan tables are uploaded once and later calls only refresh the per-call
+// region (measurement variates, status words, outcomes).
 int execute(aleph_b200_handle* h, aleph_b200_state* st, const Plan& P, const double* uniforms, uint32_t n_uniforms,
-            std::vector<int32_t>* status_out, std::vector<uint8_t>* outcomes_out) {
+            std::vector<int32_t>* status_out, std::vector<uint8_t>* outcomes_out, Scratch* cache = nullptr,
+            bool* cache_ready = nullptr) {
   const bool f64 = st->precision == ALEPH_B200_F64;
+  Scratch& buf = cache ? *cache : h->plan_buf;
+  const bool reuse = cache && cache_ready && *cache_ready;
+  if (cache && n_uniforms > P.n_measures) n_uniforms = P.n_measures;  // at most one variate per measurement
+  const uint32_t ucap = cache ? P.n_measures : n_uniforms;
   // host image of the device tables
   std::vector<float> coef32;
-  if (!f64) {
+  if (!f64 && !reuse) {
     coef32.resize(P.coef.size());
     for (size_t i = 0; i < P.coef.size(); ++i) coef32[i] = (float)P.coef[i];
   }
   const size_t b_ops = al(P.ops.size() * sizeof(Op));
-  const size_t b_coef = al(f64 ? P.coef.size() * 8 : coef32.size() * 4);
+  const size_t b_coef = al(P.coef.size() * (f64 ? 8 : 4));
   const size_t b_pa = al(P.poly_angle.size() * 8), b_po = al(P.poly_off.size() * 4), b_pc = al(P.poly_cnt.size() * 4),
                b_pd = al(P.poly_conds.size() * 8);
-  const size_t b_u = al((size_t)n_uniforms * 8), b_s = al(64), b_o = al(P.n_measures + 1);
+  const size_t b_u = al((size_t)ucap * 8), b_s = al(64), b_o = al(P.n_measures + 1);
   const size_t b_img = al(P.block_images.size());
   const size_t total = b_img + b_ops + b_coef + b_pa + b_po + b_pc + b_pd + b_u + b_s + b_o;
-  if (int r = ensure(h, h->plan_buf, total)) return r;
-  std::vector<uint8_t> img(total, 0);
+  if (int r = ensure(h, buf, total)) return r;
+  std::vector<uint8_t> img(reuse ? 0 : total, 0);
   size_t off = 0;
   auto put = [&](const void* src, size_t bytes, size_t span) -> size_t {
     const size_t at = off;
-    if (bytes) std::memcpy(img.data() + off, src, bytes);
+    if (bytes && !reuse) std::memcpy(img.data() + off, src, bytes);
     off += span;
     return at;
   };
   const size_t o_img = put(P.block_images.data(), P.block_images.size(), b_img);
   const size_t o_ops = put(P.ops.data(), P.ops.size() * sizeof(Op), b_ops);
-  const size_t o_coef = f64 ? put(P.coef.data(), P.coef.size() * 8, b_coef) : put(coef32.data(), coef32.size() * 4, b_coef);
+  const size_t o_coef = f64 ? put(P.coef.data(), P.coef.size() * 8, b_coef) : put(coef32.data(), P.coef.size() * 4, b_coef);
   const size_t o_pa = put(P.poly_angle.data(), P.poly_angle.size() * 8, b_pa);
   const size_t o_po = put(P.poly_off.data(), P.poly_off.size() * 4, b_po);
   const size_t o_pc = put(P.poly_cnt.data(), P.poly_cnt.size() * 4, b_pc);
@@ -183,8 +200,16 @@ int execute(aleph_b200_handle* h, aleph_b200_state* st, const Plan& P, const dou
   const size_t o_u = put(uniforms, (size_t)n_uniforms * 8, b_u);
   const size_t o_s = put(nullptr, 0, b_s);
   const size_t o_o = put(nullptr, 0, b_o);
-  CK(cudaMemcpyAsync(h->plan_buf.ptr, img.data(), total, cudaMemcpyHostToDevice, h->stream), "plan upload");
-  char* base = (char*)h->plan_buf.ptr;
+  char* base = (char*)buf.ptr;
+  if (!reuse) {
+    CK(copy_async(h, buf.ptr, img.data(), total, cudaMemcpyHostToDevice, h->stream), "plan upload");
+  } else {
+    if (n_uniforms)
+      CK(copy_async(h, base + o_u, uniforms, (size_t)n_uniforms * 8, cudaMemcpyHostToDevice, h->stream),
+         "variates upload");
+    CK(cudaMemsetAsync(base + o_s, 0, b_s + b_o, h->stream), "status clear");
+  }
+  if (cache_ready) *cache_ready = true;
   DevPlan d;
   d.ops = (Op*)(base + o_ops);
   d.coef = base + o_coef;
@@ -302,10 +327,10 @@ int execute(aleph_b200_handle* h, aleph_b200_state* st, const Plan& P, const dou
   }
   if (status_out || outcomes_out || P.n_measures || any_block) {
     std::vector<int32_t> stv(16, 0);
-    CK(cudaMemcpyAsync(stv.data(), d.status, 16 * 4, cudaMemcpyDeviceToHost, h->stream), "status readback");
+    CK(copy_async(h, stv.data(), d.status, 16 * 4, cudaMemcpyDeviceToHost, h->stream), "status readback");
     std::vector<uint8_t> oc(P.n_measures + 1, 0);
     if (P.n_measures)
-      CK(cudaMemcpyAsync(oc.data(), d.outcomes, P.n_measures, cudaMemcpyDeviceToHost, h->stream), "outcome readback");
+      CK(copy_async(h, oc.data(), d.outcomes, P.n_measures, cudaMemcpyDeviceToHost, h->stream), "outcome readback");
     CK(cudaStreamSynchronize(h->stream), "stream synchronize");
     if (stv[4] != 0)  // a tensor-core block pass gave up on a bounded wait
       return set_error(h, ALEPH_B200_DEVICE_FAILURE, "device operation failed: block pass wait expired");
@@ -414,6 +439,14 @@ int aleph_b200_free_state(aleph_b200_handle* h, aleph_b200_state* st) {
   return ALEPH_B200_OK;
 }
 
+int aleph_b200_reset_state(aleph_b200_handle* h, aleph_b200_state* st) {
+  if (!h || !st) return ALEPH_B200_INVALID_ARGUMENT;
+  if (int r = bind(h)) return r;
+  CK(launch_init_zero_state(st->amps, st->n, st->precision, h->stream), "state init");
+  h->stats.kernel_launches++;
+  return ALEPH_B200_OK;
+}
+
 int aleph_b200_num_qubits(const aleph_b200_state* st, uint32_t* out) {
   if (!st || !out) return ALEPH_B200_INVALID_ARGUMENT;
   *out = st->n;
@@ -438,15 +471,13 @@ int aleph_b200_apply_gate(aleph_b200_handle* h, aleph_b200_state* st, const alep
   return execute(h, st, P, nullptr, 0, nullptr, nullptr);
 }
 
-static int stream_impl(aleph_b200_handle* h, aleph_b200_state* st, const aleph_b200_instr* in, uint64_t count,
-                       const aleph_b200_pools* pools, const double* mu, uint64_t n_mu, uint8_t* outcomes,
-                       uint64_t outcomes_cap, uint64_t* n_outcomes, int32_t* used_out) {
-  if (!h || !st || (!in && count)) return ALEPH_B200_INVALID_ARGUMENT;
-  if (int r = bind(h)) return r;
-  if (n_outcomes) *n_outcomes = 0;
+// Lowers a record stream for an n-qubit register into planner ops, validating
+// every record first (crates/aleph-sv/src/backend.rs apply_gate order).
+static int lower_stream(aleph_b200_handle* h, uint32_t n, const aleph_b200_instr* in, uint64_t count,
+                        const aleph_b200_pools* pools, std::vector<Lowered>* out) {
   const double* pool = pools ? pools->matrix_pool : nullptr;
   const uint64_t pool_len = pools ? pools->matrix_pool_len : 0;
-  std::vector<Lowered> ops;
+  std::vector<Lowered>& ops = *out;
   ops.reserve(count);
   for (uint64_t i = 0; i < count; ++i) {
     const aleph_b200_instr& g = in[i];
@@ -454,7 +485,7 @@ static int stream_impl(aleph_b200_handle* h, aleph_b200_state* st, const aleph_b
     e.instruction = (uint32_t)i;
     if (g.kind < 28) {
       ops.emplace_back();
-      if (lower_gate(g, st->n, pool, pool_len, &ops.back(), &e)) return report(h, e);
+      if (lower_gate(g, n, pool, pool_len, &ops.back(), &e)) return report(h, e);
       ops.back().record = (uint32_t)i;
     } else if (g.kind == ALEPH_INSTR_MEASURE) {
       if (g.num_qubits != 1) {
@@ -462,10 +493,10 @@ static int stream_impl(aleph_b200_handle* h, aleph_b200_state* st, const aleph_b
         std::snprintf(e.kind, sizeof(e.kind), "measure record");
         return report(h, e);
       }
-      if (g.qubits[0] >= st->n) {
+      if (g.qubits[0] >= n) {
         e.status = ALEPH_B200_QUBIT_OUT_OF_RANGE;
         e.qubit = g.qubits[0];
-        e.num_qubits = st->n;
+        e.num_qubits = n;
         return report(h, e);
       }
       ops.emplace_back();
@@ -496,9 +527,14 @@ static int stream_impl(aleph_b200_handle* h, aleph_b200_state* st, const aleph_b
       return report(h, e);
     }
   }
-  Plan P;
-  if (int s = build_plan(ops, st->n, h->opts, &P)) return set_error(h, s, "optimization pipeline failed: planner");
-  // measurement variates: explicit, or drawn from the handle RNG (only the consumed ones advance it)
+  return ALEPH_B200_OK;
+}
+
+// Runs a lowered plan with measurement variates: explicit, or drawn from the
+// handle RNG (only the consumed ones advance it).
+static int run_plan(aleph_b200_handle* h, aleph_b200_state* st, const Plan& P, const double* mu, uint64_t n_mu,
+                    uint8_t* outcomes, uint64_t outcomes_cap, uint64_t* n_outcomes, int32_t* used_out,
+                    Scratch* cache = nullptr, bool* cache_ready = nullptr) {
   std::vector<double> drawn;
   uint64_t saved[4];
   std::memcpy(saved, ext(h)->rng, sizeof(saved));
@@ -510,7 +546,7 @@ static int stream_impl(aleph_b200_handle* h, aleph_b200_state* st, const aleph_b
   }
   std::vector<int32_t> stv;
   std::vector<uint8_t> oc;
-  if (int r = execute(h, st, P, mu, (uint32_t)n_mu, &stv, &oc)) return r;
+  if (int r = execute(h, st, P, mu, (uint32_t)n_mu, &stv, &oc, cache, cache_ready)) return r;
   if (!drawn.empty()) {
     std::memcpy(ext(h)->rng, saved, sizeof(saved));
     for (int32_t k = 0; k < stv[1]; ++k) rng_next(h);
@@ -532,10 +568,77 @@ static int stream_impl(aleph_b200_handle* h, aleph_b200_state* st, const aleph_b
   return ALEPH_B200_OK;
 }
 
+static int stream_impl(aleph_b200_handle* h, aleph_b200_state* st, const aleph_b200_instr* in, uint64_t count,
+                       const aleph_b200_pools* pools, const double* mu, uint64_t n_mu, uint8_t* outcomes,
+                       uint64_t outcomes_cap, uint64_t* n_outcomes, int32_t* used_out) {
+  if (!h || !st || (!in && count)) return ALEPH_B200_INVALID_ARGUMENT;
+  if (int r = bind(h)) return r;
+  if (n_outcomes) *n_outcomes = 0;
+  std::vector<Lowered> ops;
+  if (int r = lower_stream(h, st->n, in, count, pools, &ops)) return r;
+  Plan P;
+  if (int s = build_plan(ops, st->n, h->opts, &P)) return set_error(h, s, "optimization pipeline failed: planner");
+  return run_plan(h, st, P, mu, n_mu, outcomes, outcomes_cap, n_outcomes, used_out);
+}
+
 int aleph_b200_apply_gate_stream(aleph_b200_handle* h, aleph_b200_state* st, const aleph_b200_instr* in, uint64_t count,
                                  const aleph_b200_pools* pools, const double* mu, uint64_t n_mu, uint8_t* outcomes,
                                  uint64_t outcomes_cap, uint64_t* n_outcomes) {
   return stream_impl(h, st, in, count, pools, mu, n_mu, outcomes, outcomes_cap, n_outcomes, nullptr);
+}
+
+struct aleph_b200_plan {
+  uint32_t n = 0;
+  Plan P;
+  Scratch buf;
+  bool uploaded = false;
+};
+
+int aleph_b200_compile(aleph_b200_handle* h, uint32_t num_qubits, const aleph_b200_instr* in, uint64_t count,
+                       const aleph_b200_pools* pools, aleph_b200_plan** out) {
+  if (!h || !out || (!in && count)) return ALEPH_B200_INVALID_ARGUMENT;
+  *out = nullptr;
+  if (num_qubits > h->qubit_cap || num_qubits > 40) {
+    aleph_b200_error_info e{};
+    e.status = ALEPH_B200_TOO_MANY_QUBITS;
+    e.requested = num_qubits;
+    e.limit = h->qubit_cap;
+    return report(h, e);
+  }
+  std::vector<Lowered> ops;
+  if (int r = lower_stream(h, num_qubits, in, count, pools, &ops)) return r;
+  aleph_b200_plan* p = new (std::nothrow) aleph_b200_plan();
+  if (!p) return set_error(h, ALEPH_B200_DEVICE_FAILURE, "host allocation failed");
+  p->n = num_qubits;
+  if (int s = build_plan(ops, num_qubits, h->opts, &p->P)) {
+    delete p;
+    return set_error(h, s, "optimization pipeline failed: planner");
+  }
+  *out = p;
+  return ALEPH_B200_OK;
+}
+
+int aleph_b200_execute(aleph_b200_handle* h, aleph_b200_state* st, aleph_b200_plan* plan, const double* mu,
+                       uint64_t n_mu, uint8_t* outcomes, uint64_t outcomes_cap, uint64_t* n_outcomes) {
+  if (!h || !st || !plan) return ALEPH_B200_INVALID_ARGUMENT;
+  if (n_outcomes) *n_outcomes = 0;
+  if (plan->n != st->n)
+    return set_error(h, ALEPH_B200_INVALID_ARGUMENT, "plan compiled for %u qubits, state has %u", plan->n, st->n);
+  if (int r = bind(h)) return r;
+  return run_plan(h, st, plan->P, mu, n_mu, outcomes, outcomes_cap, n_outcomes, nullptr, &plan->buf, &plan->uploaded);
+}
+
+int aleph_b200_plan_free(aleph_b200_handle* h, aleph_b200_plan* plan) {
+  if (!plan) return ALEPH_B200_OK;
+  if (plan->buf.ptr) {
+    if (h) {
+      cudaSetDevice(h->device);
+      cudaStreamSynchronize(h->stream);
+    }
+    cudaFree(plan->buf.ptr);
+  }
+  delete plan;
+  return ALEPH_B200_OK;
 }
 
 int aleph_b200_apply_diagonal_phase(aleph_b200_handle* h, aleph_b200_state* st, const aleph_b200_phase_term* terms,
@@ -564,7 +667,7 @@ int aleph_b200_unpermute(aleph_b200_handle* h, aleph_b200_state* st, const uint3
   CK(cudaMalloc(&tmp, st->bytes), "unpermute buffer");
   uint32_t* dperm = nullptr;
   cudaError_t e = cudaMalloc(&dperm, 64 * 4);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(dperm, perm, n * 4, cudaMemcpyHostToDevice, h->stream);
+  if (e == cudaSuccess) e = copy_async(h, dperm, perm, n * 4, cudaMemcpyHostToDevice, h->stream);
   if (e == cudaSuccess) e = launch_unpermute(st->amps, tmp, st->precision, n, dperm, h->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
   if (e != cudaSuccess) {
@@ -612,7 +715,7 @@ static int check_norm_host(aleph_b200_handle* h, aleph_b200_state* st, double* n
   CK(launch_norm(st->amps, st->precision, st->n, part, nb, out2, h->stream), "norm");
   h->stats.kernel_launches += 2;
   double res[2];
-  CK(cudaMemcpyAsync(res, out2, 16, cudaMemcpyDeviceToHost, h->stream), "norm readback");
+  CK(copy_async(h, res, out2, 16, cudaMemcpyDeviceToHost, h->stream), "norm readback");
   CK(cudaStreamSynchronize(h->stream), "stream synchronize");
   if (norm_out) *norm_out = res[0];
   const double len = (double)(1ull << st->n);
@@ -650,13 +753,13 @@ int aleph_b200_sample(aleph_b200_handle* h, aleph_b200_state* st, uint32_t shots
   int32_t* dstatus = (int32_t*)(base + al(sb) + 2 * al(vb));
   CK(cudaMemsetAsync(dstatus, 0, 64, h->stream), "status clear");
   CK(cudaMemsetAsync(base, 0, sb, h->stream), "scratch clear");
-  CK(cudaMemcpyAsync(dvar, variates, vb, cudaMemcpyHostToDevice, h->stream), "variates upload");
+  CK(copy_async(h, dvar, variates, vb, cudaMemcpyHostToDevice, h->stream), "variates upload");
   CK(launch_sample(st->amps, st->precision, st->n, shots, mode, dvar, dout, base, sb, dstatus, h->sm_count, h->stream),
      "sample");
   h->stats.kernel_launches += mode == ALEPH_B200_SAMPLE_ALIAS ? 7 : 5;
   int32_t status[4];
-  CK(cudaMemcpyAsync(status, dstatus, 16, cudaMemcpyDeviceToHost, h->stream), "status readback");
-  CK(cudaMemcpyAsync(out, dout, vb, cudaMemcpyDeviceToHost, h->stream), "sample readback");
+  CK(copy_async(h, status, dstatus, 16, cudaMemcpyDeviceToHost, h->stream), "status readback");
+  CK(copy_async(h, out, dout, vb, cudaMemcpyDeviceToHost, h->stream), "sample readback");
   CK(cudaStreamSynchronize(h->stream), "stream synchronize");
   if (status[0]) {
     aleph_b200_error_info e{};
@@ -709,7 +812,7 @@ int aleph_b200_expectation(aleph_b200_handle* h, aleph_b200_state* st, const uin
      "expectation");
   h->stats.kernel_launches += 2;
   double res[3];
-  CK(cudaMemcpyAsync(res, out3, 24, cudaMemcpyDeviceToHost, h->stream), "expectation readback");
+  CK(copy_async(h, res, out3, 24, cudaMemcpyDeviceToHost, h->stream), "expectation readback");
   CK(cudaStreamSynchronize(h->stream), "stream synchronize");
   // validate_state first (measure.rs:166), then coefficient, then qubits (measure.rs:172-193)
   const double len = (double)(1ull << st->n);
@@ -777,12 +880,12 @@ int aleph_b200_probabilities(aleph_b200_handle* h, aleph_b200_state* st, const u
   if (int r = ensure(h, h->sample, dim * 8 + 256)) return r;
   uint32_t* dq = nullptr;
   CK(cudaMalloc(&dq, 64 * 4), "qubit list");
-  cudaError_t e = cudaMemcpyAsync(dq, qubits, k * 4, cudaMemcpyHostToDevice, h->stream);
+  cudaError_t e = copy_async(h, dq, qubits, k * 4, cudaMemcpyHostToDevice, h->stream);
   double* dout = (double*)h->sample.ptr;
   double* dnorm = dout + dim;
   if (e == cudaSuccess)
     e = launch_probabilities(st->amps, st->precision, st->n, dq, k, (double*)h->reduce.ptr, nb, dout, dnorm, h->stream);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(out, dout, dim * 8, cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = copy_async(h, out, dout, dim * 8, cudaMemcpyDeviceToHost, h->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
   cudaFree(dq);
   if (e != cudaSuccess) return cuda_fail(h, e, "probabilities");
@@ -795,12 +898,12 @@ int aleph_b200_get_amplitudes(aleph_b200_handle* h, aleph_b200_state* st, double
   if (int r = bind(h)) return r;
   const uint64_t len = 1ull << st->n;
   if (st->precision == ALEPH_B200_F64) {
-    CK(cudaMemcpyAsync(out, st->amps, st->bytes, cudaMemcpyDeviceToHost, h->stream), "amplitude readback");
+    CK(copy_async(h, out, st->amps, st->bytes, cudaMemcpyDeviceToHost, h->stream), "amplitude readback");
     CK(cudaStreamSynchronize(h->stream), "stream synchronize");
     return ALEPH_B200_OK;
   }
   std::vector<float> tmp(2 * len);
-  CK(cudaMemcpyAsync(tmp.data(), st->amps, st->bytes, cudaMemcpyDeviceToHost, h->stream), "amplitude readback");
+  CK(copy_async(h, tmp.data(), st->amps, st->bytes, cudaMemcpyDeviceToHost, h->stream), "amplitude readback");
   CK(cudaStreamSynchronize(h->stream), "stream synchronize");
   for (uint64_t i = 0; i < 2 * len; ++i) out[i] = tmp[i];
   return ALEPH_B200_OK;
@@ -811,13 +914,13 @@ int aleph_b200_set_amplitudes(aleph_b200_handle* h, aleph_b200_state* st, const 
   if (int r = bind(h)) return r;
   const uint64_t len = 1ull << st->n;
   if (st->precision == ALEPH_B200_F64) {
-    CK(cudaMemcpyAsync(st->amps, in, st->bytes, cudaMemcpyHostToDevice, h->stream), "amplitude upload");
+    CK(copy_async(h, st->amps, in, st->bytes, cudaMemcpyHostToDevice, h->stream), "amplitude upload");
     CK(cudaStreamSynchronize(h->stream), "stream synchronize");
     return ALEPH_B200_OK;
   }
   std::vector<float> tmp(2 * len);
   for (uint64_t i = 0; i < 2 * len; ++i) tmp[i] = (float)in[i];
-  CK(cudaMemcpyAsync(st->amps, tmp.data(), st->bytes, cudaMemcpyHostToDevice, h->stream), "amplitude upload");
+  CK(copy_async(h, st->amps, tmp.data(), st->bytes, cudaMemcpyHostToDevice, h->stream), "amplitude upload");
   CK(cudaStreamSynchronize(h->stream), "stream synchronize");
   return ALEPH_B200_OK;
 }
@@ -832,9 +935,15 @@ int aleph_b200_norm_sqr(aleph_b200_handle* h, aleph_b200_state* st, double* out)
   CK(launch_norm(st->amps, st->precision, st->n, part, nb, out2, h->stream), "norm");
   h->stats.kernel_launches += 2;
   double res[2];
-  CK(cudaMemcpyAsync(res, out2, 16, cudaMemcpyDeviceToHost, h->stream), "norm readback");
+  CK(copy_async(h, res, out2, 16, cudaMemcpyDeviceToHost, h->stream), "norm readback");
   CK(cudaStreamSynchronize(h->stream), "stream synchronize");
   *out = res[1] > 0.0 ? NAN : res[0];
+  return ALEPH_B200_OK;
+}
+
+int aleph_b200_get_stream(const aleph_b200_handle* h, void** stream) {
+  if (!h || !stream) return ALEPH_B200_INVALID_ARGUMENT;
+  *stream = (void*)h->stream;
   return ALEPH_B200_OK;
 }
 

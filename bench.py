@@ -1,0 +1,458 @@
+"""Benchmark of the dense state-vector hot path on B200.
+
+Workload: the random brickwall circuit at n=32 qubits, depth 40 (every layer
+a Haar-random SU(2) on each qubit, then CZ on nearest-neighbour pairs with
+alternating even/odd offsets), starting from |0...0>, run in the
+tensor-core FP32 form (complex64 state, fused 6-qubit blocks as split-BF16x3
+tcgen05 GEMMs with FP32 accumulation). The same circuit on this engine's
+plain FP64 path is timed beside it, and the TC-FP32 state is compared with
+the FP64 state on an n=28 copy of the circuit.
+
+One step = one circuit: reset of the 32 GiB state to |0...0> plus every pass
+of the compiled plan (plan tables resident on the device). The state is far
+larger than the 126 MB L2, so no flush is needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
+
+N > 1 runs one independent replica per GPU (the path does not shard; there
+is no data-path collective): `value` is the job's wall time per circuit,
+max-over-ranks device time / circuits run by all ranks.
+
+`--impl reference` times the CPU restatement of the reference `sv` FP64
+backend (oracle/) on the host cores, on a bounded sample of the same
+circuit, extrapolated to the full workload per gate and amplitude.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "circuit wall time & HBM % of peak, n=32 brickwall: TC-FP32 vs plain FP64"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def host_cores() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def measured_hbm_peak() -> tuple[float, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    try:
+        v = float(json.loads(p.read_text())["hbm_gbs"])
+        return v, "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def workload_name(n: int, depth: int) -> str:
+    return (f"random brickwall n={n} depth={depth} (Haar SU(2) on every qubit + CZ on alternating "
+            f"nearest-neighbour pairs), |0...0> start")
+
+
+FORMS = {
+    "tc32": "TC-FP32: complex64 state, fused 6-qubit blocks on tcgen05 (split-BF16x3 operands, FP32 accumulate)",
+    "f32": "FP32: complex64 state on CUDA cores",
+    "f64": "plain FP64: complex128 state on CUDA cores",
+}
+
+
+def base_config(args, gates: int) -> dict:
+    return {"workload": workload_name(args.n, args.depth), "n": args.n, "depth": args.depth, "gates": gates,
+            "seed": args.seed, "form": FORMS[args.precision],
+            "l2": f"inputs larger than L2: {float(1 << args.n) * 8 / 2**30:.0f} GiB complex64 state, no flush",
+            "step": "reset to |0..0> + compiled plan (tables resident)"}
+
+
+def brickwall_gates(n: int, depth: int) -> int:
+    return n * depth + sum(len(range(layer % 2, n - 1, 2)) for layer in range(depth))
+
+
+# ---- clocks sampled during the timed region ----------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines: list[str] = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---- distributed plumbing (replicas only) -------------------------------------
+class Ranks:
+    def __init__(self):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = False
+
+    def init(self):
+        if self.world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as dist
+
+            torch.cuda.set_device(self.local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                    device_id=torch.device("cuda", self.local))
+            self.pg = True
+
+    def barrier(self):
+        if self.pg:
+            import torch.distributed as dist
+
+            dist.barrier()
+
+    def max(self, x: float) -> float:
+        if not self.pg:
+            return x
+        import torch
+        import torch.distributed as dist
+
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{self.local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+# ---- CPU baseline: the oracle on a bounded sample -----------------------------
+def cpu_sample_seconds(n_full: int, depth_full: int, n_sample: int, layers: int) -> tuple[float, str]:
+    """Times the oracle (CPU restatement of the reference sv FP64 backend) on
+    the first `layers` layers of the brickwall at n_sample qubits and scales
+    per gate and amplitude to the full circuit; returns (s/circuit, sample)."""
+    from aleph_b200 import workloads
+    from oracle import oracle
+
+    c = workloads.brickwall(n_sample, layers, seed=0)
+    gates = len(c.instructions)
+    oracle.run(n_sample, c.instructions[: n_sample])  # page-in, thread start-up
+    t0 = time.perf_counter()
+    oracle.run(n_sample, c.instructions)
+    dt = time.perf_counter() - t0
+    per_gate_amp = dt / (gates * float(1 << n_sample))
+    full = per_gate_amp * brickwall_gates(n_full, depth_full) * float(1 << n_full)
+    sample = (f"oracle FP64 (CPU restatement of the reference sv backend, per-gate sweeps) on the first "
+              f"{layers} layers ({gates} gates) of the brickwall at n={n_sample}: {dt:.2f} s, "
+              f"{per_gate_amp * 1e9:.3f} ns per gate-amplitude, scaled to "
+              f"{brickwall_gates(n_full, depth_full)} gates x 2^{n_full} amplitudes")
+    return full, sample
+
+
+def run_reference(args, ranks: Ranks):
+    if ranks.rank != 0:
+        return 0
+    cores = host_cores()
+    os.environ.setdefault("ORACLE_THREADS", str(cores))
+    vals = []
+    sample = ""
+    for i in range(args.warmup + args.steps):
+        v, sample = cpu_sample_seconds(args.n, args.depth, args.ref_sample_n, 2)
+        if i >= args.warmup:
+            vals.append(v)
+    value = statistics.median(vals)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": dict(base_config(args, brickwall_gates(args.n, args.depth)),
+                       parallelism="host threads (rank 0)", timed="CPU restatement of the reference sv FP64 backend"),
+        "cpu_baseline": {"value": value, "unit": "s", "cores": int(os.environ["ORACLE_THREADS"]), "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---- the engine arm ---------------------------------------------------------------
+def time_plan(be, plan, st, steps: int, warmup: int, ranks: Ranks, record: bool, clocks: ClockSampler | None):
+    """Device time of `steps` circuits (reset + plan) on the engine stream."""
+    import torch
+
+    stream = torch.cuda.ExternalStream(be.stream_ptr())
+    for _ in range(warmup):
+        be.reset_state(st)
+        plan.execute(st)
+    be.synchronize()
+    be.set_tuning("record_passes", 1 if record else 0)
+    per_pass: list[dict] = []
+    l0 = be.stats()
+    ranks.barrier()
+    torch.cuda.synchronize()
+    if clocks:
+        clocks.start()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(steps):
+        be.reset_state(st)
+        plan.execute(st)
+        if record:
+            per_pass.extend(be.pass_records())
+    ev1.record(stream)
+    ev1.synchronize()
+    torch.cuda.synchronize()
+    ranks.barrier()
+    clk = clocks.stop() if clocks else None
+    be.set_tuning("record_passes", 0)
+    l1 = be.stats()
+    ms = ev0.elapsed_time(ev1)
+    return ms, per_pass, l1["kernel_launches"] - l0["kernel_launches"], clk
+
+
+def kernel_table(per_pass: list[dict], peak: float) -> dict:
+    kinds: dict[str, dict] = {}
+    for r in per_pass:
+        k = kinds.setdefault(r["kind"], {"launches": 0, "ms": 0.0, "bytes": 0.0})
+        k["launches"] += 1
+        k["ms"] += r["ms"]
+        k["bytes"] += r["bytes"]
+    total = sum(k["ms"] for k in kinds.values()) or 1.0
+    out = {}
+    for name, k in kinds.items():
+        gbs = k["bytes"] / (k["ms"] * 1e-3) / 1e9 if k["ms"] > 0 else 0.0
+        out[name] = {"launches": k["launches"], "ms_total": round(k["ms"], 4), "share": round(k["ms"] / total, 4),
+                     "ms_per_launch": round(k["ms"] / k["launches"], 5), "gbs": round(gbs, 1),
+                     "frac_of_peak": round(gbs / peak, 4)}
+    return out
+
+
+def fidelity_check(n: int, depth: int, seed: int) -> dict:
+    """TC-FP32 vs this engine's FP64 path on the same circuit (the FP64 path is
+    the one held to max|dpsi| <= 1e-12 against the FP64 oracle)."""
+    from aleph_b200 import workloads
+    from aleph_b200.backend import B200SvBackend
+
+    c = workloads.brickwall(n, depth, seed=seed)
+    out = {}
+    for prec in ("f64", "tc32"):
+        be = B200SvBackend(seed=0, precision=prec)
+        st = be.allocate(n)
+        be.apply_stream(st, c.instructions)
+        out[prec] = be.statevector(st)
+        st.free()
+        be.close()
+    a, b = out["f64"], out["tc32"]
+    f = abs(np.vdot(a, b)) ** 2 / (np.vdot(a, a).real * np.vdot(b, b).real)
+    return {"n": n, "depth": depth, "max_abs_dpsi": float(np.abs(a - b).max()), "one_minus_fidelity": float(1.0 - f),
+            "against": "this engine's FP64 path (held to 1e-12 of the FP64 oracle by the parity tests)"}
+
+
+def run_engine(args, ranks: Ranks):
+    import torch
+
+    from aleph_b200 import workloads
+    from aleph_b200.backend import B200SvBackend
+    from aleph_b200.circuit import flatten
+
+    ranks.init()
+    dev = ranks.local
+    torch.cuda.set_device(dev)
+    peak, peak_kind = measured_hbm_peak()
+    n, depth = args.n, args.depth
+    circ = workloads.brickwall(n, depth, seed=args.seed)
+    flat = flatten(circ.instructions)
+
+    # -- TC-FP32, device-resident: the headline value
+    be = B200SvBackend(seed=args.seed, device=dev, precision=args.precision)
+    plan = be.compile(n, flat)
+    st = be.allocate(n)
+    clocks = ClockSampler(dev)
+    ms, per_pass, launches, clk = time_plan(be, plan, st, args.steps, args.warmup, ranks, True, clocks)
+    ms_max = ranks.max(ms)
+    norm = be.norm_sqr(st)
+    s_per_circuit = ms_max * 1e-3 / (args.steps * ranks.world)
+    table = kernel_table(per_pass, peak)
+    # dominant kernel and its roofline (algorithmic bytes per launch / mean launch time)
+    dom = max(table, key=lambda k: table[k]["ms_total"]) if table else None
+    roof = None
+    if dom:
+        d = table[dom]
+        algo_per_launch = 2.0 * float(1 << n) * (16.0 if args.precision == "f64" else 8.0)
+        if dom == "measure":
+            algo_per_launch *= 1.5
+        achieved = algo_per_launch / (d["ms_per_launch"] * 1e-3) / 1e9
+        traffic = TRAFFIC_PER_AMP.get((args.precision, dom))
+        roof = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                "traffic": None if traffic is None else traffic * float(1 << n),
+                "algorithmic_bytes_per_launch": algo_per_launch}
+    plan.free()
+
+    # -- end to end through the C ABI with host buffers: allocate, the gate
+    #    stream from host records (validation, planning, plan upload), 1024
+    #    shots back to the host, free
+    shots = 1024
+    rng = np.random.default_rng(args.seed)
+    variates = rng.random(shots)
+    st.free()
+
+    def e2e_step():
+        s = be.allocate(n)
+        be.apply_stream(s, None, flat=flat)
+        out = be.sample(s, shots, variates=variates, mode="cumulative")
+        s.free()
+        return out
+
+    for _ in range(max(1, args.e2e_warmup)):
+        e2e_step()
+    be.synchronize()
+    s0 = be.stats()
+    ranks.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        e2e_step()
+    be.synchronize()
+    t1 = time.perf_counter()
+    ranks.barrier()
+    s1 = be.stats()
+    e2e_s = ranks.max(t1 - t0) / (args.e2e_steps * ranks.world)
+    e2e = {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": (s1["h2d_bytes"] - s0["h2d_bytes"]) // args.e2e_steps,
+           "d2h_bytes_per_step": (s1["d2h_bytes"] - s0["d2h_bytes"]) // args.e2e_steps,
+           "steps": args.e2e_steps, "what": "allocate + apply_gate_stream(host records) + 1024 shots to host + free"}
+    be.close()
+
+    # -- the plain FP64 path on the same circuit
+    fp64 = None
+    if not args.skip_fp64:
+        b64 = B200SvBackend(seed=args.seed, device=dev, precision="f64")
+        p64 = b64.compile(n, flat)
+        s64 = b64.allocate(n)
+        ms64, per64, _, _ = time_plan(b64, p64, s64, args.fp64_steps, max(3, args.warmup), ranks, True, None)
+        ms64 = ranks.max(ms64)
+        s64_per = ms64 * 1e-3 / (args.fp64_steps * ranks.world)
+        fp64 = {"s_per_circuit": s64_per, "steps": args.fp64_steps, "tc32_speedup": s64_per / s_per_circuit,
+                "kernels": kernel_table(per64, peak)}
+        p64.free()
+        s64.free()
+        b64.close()
+
+    fid = None
+    if args.fidelity_n and ranks.rank == 0:
+        fid = fidelity_check(args.fidelity_n, depth, args.seed)
+
+    cpu = None
+    if ranks.world == 1 and not args.skip_cpu:
+        cores = host_cores()
+        os.environ.setdefault("ORACLE_THREADS", str(cores))
+        v, sample = cpu_sample_seconds(n, depth, args.cpu_sample_n, 2)
+        cpu = {"value": v, "unit": "s", "cores": int(os.environ["ORACLE_THREADS"]), "kind": "port", "sample": sample}
+
+    if ranks.rank == 0:
+        line = {
+            "metric": METRIC, "value": s_per_circuit, "unit": "s", "n_gpus": ranks.world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 (tc32: split-bf16x3 tensor-core blocks, fp32 accumulate)"
+            if args.precision == "tc32" else args.precision, "data": "synthetic",
+            "config": dict(base_config(args, len(circ.instructions)),
+                           parallelism=f"replicas x{ranks.world}" if ranks.world > 1 else "single GPU"),
+            "clocks": clk, "e2e": e2e, "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu,
+            "kernels": table, "fp64_plain": fp64, "fidelity": fid, "final_norm_sqr": norm,
+        }
+        print(json.dumps(line), flush=True)
+    ranks.close()
+    return 0
+
+
+# DRAM bytes (read + write) per amplitude of one launch of the dominant
+# kernel, from an ncu capture of that kernel on a smaller register, scaled by
+# the amplitudes it processes (traffic grows in proportion to 2^n).
+TRAFFIC_PER_AMP: dict[tuple[str, str], float] = {}
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
+    ap.add_argument("--n", type=int, default=32)
+    ap.add_argument("--depth", type=int, default=40)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--precision", choices=["tc32", "f32", "f64"], default="tc32")
+    ap.add_argument("--fp64-steps", type=int, default=3)
+    ap.add_argument("--skip-fp64", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--e2e-warmup", type=int, default=1)
+    ap.add_argument("--fidelity-n", type=int, default=28)
+    ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--cpu-sample-n", type=int, default=26)
+    ap.add_argument("--ref-sample-n", type=int, default=26)
+    args = ap.parse_args(argv)
+    args.warmup = max(3, args.warmup)  # at least 3 untimed warm-up steps
+    ranks = Ranks()
+    if args.impl == "reference":
+        return run_reference(args, ranks)
+    return run_engine(args, ranks)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -184,6 +184,9 @@ int aleph_b200_set_qubit_cap(aleph_b200_handle* h, uint32_t cap);
 int aleph_b200_allocate(aleph_b200_handle* h, uint32_t num_qubits, aleph_b200_state** out);
 int aleph_b200_free_state(aleph_b200_handle* h, aleph_b200_state* st);
 int aleph_b200_num_qubits(const aleph_b200_state* st, uint32_t* out);
+/* Puts an allocated state back to |0...0> on the device (the state a fresh
+ * Backend::allocate returns), so one allocation can serve many runs. */
+int aleph_b200_reset_state(aleph_b200_handle* h, aleph_b200_state* st);
 
 /* ---- Backend::apply_gate (crates/aleph-sv/src/backend.rs:74-152) ---- */
 int aleph_b200_apply_gate(aleph_b200_handle* h, aleph_b200_state* st, const aleph_b200_instr* gate,
@@ -199,6 +202,22 @@ int aleph_b200_apply_gate_stream(aleph_b200_handle* h, aleph_b200_state* st, con
                                  uint64_t count, const aleph_b200_pools* pools, const double* measure_uniforms,
                                  uint64_t n_uniforms, uint8_t* outcomes, uint64_t outcomes_cap,
                                  uint64_t* n_outcomes);
+
+/* ---- compiled plans: CudaExecutionPlan::compile / execute
+ * (crates/aleph-cuda/src/execution.rs:57-78,183) ----
+ * aleph_b200_compile validates and plans a record stream for a
+ * `num_qubits`-qubit register of this handle once; the plan tables are
+ * uploaded to device memory at the first execute and stay resident.
+ * aleph_b200_execute then applies the plan to `st` (same qubit count) with
+ * the semantics of aleph_b200_apply_gate_stream. A plan belongs to the handle
+ * that compiled it; calls on one handle are stream-ordered. */
+typedef struct aleph_b200_plan aleph_b200_plan;
+int aleph_b200_compile(aleph_b200_handle* h, uint32_t num_qubits, const aleph_b200_instr* instrs, uint64_t count,
+                       const aleph_b200_pools* pools, aleph_b200_plan** out);
+int aleph_b200_execute(aleph_b200_handle* h, aleph_b200_state* st, aleph_b200_plan* plan,
+                       const double* measure_uniforms, uint64_t n_uniforms, uint8_t* outcomes, uint64_t outcomes_cap,
+                       uint64_t* n_outcomes);
+int aleph_b200_plan_free(aleph_b200_handle* h, aleph_b200_plan* plan);
 
 /* ---- Backend::apply_diagonal_phase (crates/aleph-sv/src/kernels/diagonal_phase.rs:74-97) ---- */
 int aleph_b200_apply_diagonal_phase(aleph_b200_handle* h, aleph_b200_state* st, const aleph_b200_phase_term* terms,
@@ -237,6 +256,10 @@ int aleph_b200_norm_sqr(aleph_b200_handle* h, aleph_b200_state* st, double* out)
 
 /* ---- stream / errors ---- */
 int aleph_b200_synchronize(aleph_b200_handle* h);
+/* The handle's CUDA stream (a cudaStream_t), on which every kernel of the
+ * handle is launched: callers time or order work against it with their own
+ * events. */
+int aleph_b200_get_stream(const aleph_b200_handle* h, void** stream);
 int aleph_b200_last_error(const aleph_b200_handle* h, char* buf, uint64_t len);
 int aleph_b200_last_error_info(const aleph_b200_handle* h, aleph_b200_error_info* out);
 
@@ -271,6 +294,8 @@ typedef struct aleph_b200_stats {
   uint64_t block_passes;      /* of which tensor-core dense-block passes            */
   uint64_t gates_planned;     /* gates consumed by the planner                      */
   double algorithmic_bytes;   /* sum of (amplitudes read + written) * bytes/amp     */
+  uint64_t h2d_bytes;         /* bytes copied host -> device (plans, variates, ...) */
+  uint64_t d2h_bytes;         /* bytes copied device -> host (results, status)      */
 } aleph_b200_stats;
 int aleph_b200_get_stats(const aleph_b200_handle* h, aleph_b200_stats* out);
 int aleph_b200_reset_stats(aleph_b200_handle* h);

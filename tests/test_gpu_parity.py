@@ -340,3 +340,26 @@ def test_tc32_qft_measure_sample():
     words = workloads.splitmix64_words(5, 512)
     assert np.array_equal(be.sample(st, 512, variates=words, mode="alias"),
                           oracle.sample_alias(be.statevector(st), words))
+
+
+# ---- compiled plans: compile once, execute many ------------------------------
+@pytest.mark.parametrize("precision", ["f64", "tc32"])
+def test_compiled_plan_matches_stream(precision):
+    n = 14
+    c = workloads.brickwall(n, 6, seed=31)
+    c.measure(2, 0)
+    c.instructions.extend(workloads.brickwall(n, 2, seed=32).instructions)
+    be = B200SvBackend(seed=0, precision=precision)
+    plan = be.compile(n, c.instructions)
+    tol = F64_TOL if precision == "f64" else TC_TOL
+    for u in (0.3, 0.9, 0.3):
+        st = be.allocate(n)
+        outs = plan.execute(st, [u])
+        want, wouts = oracle.run(n, c.instructions, uniforms=[u])
+        assert outs == wouts
+        assert np.abs(be.statevector(st) - want).max() <= tol
+        st.free()
+    st = be.allocate(n - 1)
+    with pytest.raises(Exception):
+        plan.execute(st, [0.5])
+    plan.free()
