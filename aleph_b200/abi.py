@@ -179,6 +179,8 @@ _SIGNATURES = {
     "aleph_b200_norm_sqr": ([_P, _P, ct.POINTER(ct.c_double)], ct.c_int),
     "aleph_b200_synchronize": ([_P], ct.c_int),
     "aleph_b200_get_stream": ([_P, ct.POINTER(_P)], ct.c_int),
+    "aleph_b200_sample_cumulative_noalloc": (
+        [_P, _P, ct.c_uint32, ct.POINTER(ct.c_double), ct.POINTER(ct.c_uint64)], ct.c_int),
     "aleph_b200_reset_state": ([_P, _P], ct.c_int),
     "aleph_b200_last_error": ([_P, ct.c_char_p, ct.c_uint64], ct.c_int),
     "aleph_b200_last_error_info": ([_P, ct.POINTER(ErrorInfo)], ct.c_int),

@@ -10,6 +10,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <vector>
 
@@ -779,6 +780,74 @@ int aleph_b200_sample_seeded(aleph_b200_handle* h, aleph_b200_state* st, uint32_
   }
   double u = shots ? rng_f64(h) : 0.0;
   return aleph_b200_sample(h, st, shots, ALEPH_B200_SAMPLE_CUMULATIVE, &u, out);
+}
+
+// ---- cumulative sampling from a fixed device buffer (no allocation) ------------
+// The same kernels as aleph_b200_sample(CUMULATIVE), but every device byte it
+// uses lives in one file-scope __device__ array reserved at module load
+// (kFixedSampleScratchBytes), never in the handle's grow-on-demand scratch.
+// It serves callers that cannot allocate at that point: a caller whose state
+// vectors already fill HBM (a cudaMalloc after the circuit ran would fail for
+// lack of memory), and a caller sampling resident states in a latency-bound
+// loop, where the allocating path's scratch growth (cudaFree + cudaMalloc)
+// would synchronise the whole device and stall other streams.
+namespace {
+constexpr int kMaxFixedDevices = 64;
+std::mutex g_fixed_mu;
+void* g_fixed_base[kMaxFixedDevices] = {};
+
+// Address of this device's fixed buffer; the first call per device looks it
+// up (the device is current: bind() ran before).
+int fixed_base(aleph_b200_handle* h, char** out) {
+  if (h->device < 0 || h->device >= kMaxFixedDevices)
+    return set_error(h, ALEPH_B200_INVALID_ARGUMENT, "device %d has no fixed sampling buffer", h->device);
+  std::lock_guard<std::mutex> lock(g_fixed_mu);
+  if (!g_fixed_base[h->device]) {
+    void* p = nullptr;
+    cudaError_t e = fixed_sample_scratch_address(&p);
+    if (e != cudaSuccess || !p) return cuda_fail(h, e != cudaSuccess ? e : cudaErrorInvalidSymbol, "fixed buffer address");
+    g_fixed_base[h->device] = p;
+  }
+  *out = (char*)g_fixed_base[h->device];
+  return ALEPH_B200_OK;
+}
+}  // namespace
+
+int aleph_b200_sample_cumulative_noalloc(aleph_b200_handle* h, aleph_b200_state* st, uint32_t shots,
+                                         const double* variates, uint64_t* out) {
+  if (!h || !st || (shots && (!variates || !out))) return ALEPH_B200_INVALID_ARGUMENT;
+  const size_t sb = sample_scratch_bytes(st->n, ALEPH_B200_SAMPLE_CUMULATIVE, shots);
+  const size_t vb = (size_t)shots * 8;
+  const size_t need = al(sb) + 2 * al(vb) + 256;
+  if (need > kFixedSampleScratchBytes)
+    return set_error(h, ALEPH_B200_INVALID_ARGUMENT,
+                     "fixed sampling buffer holds %zu bytes; n=%u with %u shots needs %zu (n <= 30 fits up to 65536 shots)",
+                     (size_t)kFixedSampleScratchBytes, st->n, shots, need);
+  if (int r = bind(h)) return r;
+  char* base = nullptr;
+  if (int r = fixed_base(h, &base)) return r;
+  void* dvar = base + al(sb);
+  uint64_t* dout = (uint64_t*)(base + al(sb) + al(vb));
+  int32_t* dstatus = (int32_t*)(base + al(sb) + 2 * al(vb));
+  // what must start at zero: the status words and the sampler's scratch
+  CK(cudaMemsetAsync(dstatus, 0, 64, h->stream), "status clear");
+  CK(cudaMemsetAsync(base, 0, sb, h->stream), "scratch clear");
+  if (shots) CK(copy_async(h, dvar, variates, vb, cudaMemcpyHostToDevice, h->stream), "variates upload");
+  CK(launch_sample(st->amps, st->precision, st->n, shots, ALEPH_B200_SAMPLE_CUMULATIVE, dvar, dout, base, sb, dstatus,
+                   h->sm_count, h->stream),
+     "sample");
+  h->stats.kernel_launches += shots ? 5 : 3;
+  int32_t status[4];
+  CK(copy_async(h, status, dstatus, 16, cudaMemcpyDeviceToHost, h->stream), "status readback");
+  if (shots) CK(copy_async(h, out, dout, vb, cudaMemcpyDeviceToHost, h->stream), "sample readback");
+  CK(cudaStreamSynchronize(h->stream), "stream synchronize");
+  if (status[0]) {
+    aleph_b200_error_info e{};
+    e.status = status[0];
+    std::snprintf(e.kind, sizeof(e.kind), "state norm2 deviates from 1");
+    return report(h, e);
+  }
+  return ALEPH_B200_OK;
 }
 
 int aleph_b200_expectation(aleph_b200_handle* h, aleph_b200_state* st, const uint32_t* qubits, const uint8_t* paulis,

@@ -200,6 +200,11 @@ size_t sample_scratch_bytes(uint32_t n, int mode, uint32_t shots);
 cudaError_t launch_sample(const void* amps, int precision, uint32_t n, uint32_t shots, int mode, const void* variates_dev,
                           uint64_t* out_dev, void* scratch, size_t scratch_bytes, int32_t* status, int sm_count,
                           cudaStream_t s);
+// Fixed device buffer of aleph_b200_sample_cumulative_noalloc: a file-scope
+// __device__ array of this many bytes; its address is looked up with
+// cudaGetSymbolAddress, with the target device current.
+constexpr size_t kFixedSampleScratchBytes = (size_t)8 << 20;
+cudaError_t fixed_sample_scratch_address(void** out);
 
 // Split-BF16 hi/lo operand images of a 128x128 real matrix (kernels_block.cu), 64 KiB.
 void build_block_image(const double* W, uint8_t* out);

@@ -404,4 +404,14 @@ cudaError_t launch_sample(const void* amps, int precision, uint32_t n, uint32_t 
   return cudaGetLastError();
 }
 
+// ---- fixed scratch of aleph_b200_sample_cumulative_noalloc ----------------------
+// Reserved when this module is loaded on a device, so the entry point that
+// uses it never allocates. One copy per device; calls that overlap on one
+// device share it.
+static __device__ __align__(256) unsigned char g_fixed_sample_scratch[kFixedSampleScratchBytes];
+
+cudaError_t fixed_sample_scratch_address(void** out) {
+  return cudaGetSymbolAddress(out, g_fixed_sample_scratch);
+}
+
 }  // namespace ab

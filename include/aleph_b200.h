@@ -239,6 +239,24 @@ int aleph_b200_sample(aleph_b200_handle* h, aleph_b200_state* st, uint32_t shots
 /* Same, with variates drawn from the handle's RNG (AUTO rule). */
 int aleph_b200_sample_seeded(aleph_b200_handle* h, aleph_b200_state* st, uint32_t shots, uint64_t* out);
 
+/* CUMULATIVE sampling that allocates nothing. No counterpart in the reference.
+ * Same kernels and results as aleph_b200_sample(..., ALEPH_B200_SAMPLE_CUMULATIVE,
+ * ...), but all device scratch lives in one fixed 8 MiB buffer reserved when
+ * the library's module loads on a device (no cudaMalloc / cudaFree), for
+ * callers that cannot allocate at that point: state vectors that already fill
+ * HBM, or latency-bound sampling loops where scratch growth would synchronise
+ * the device.
+ *  - Limit: the scratch of (n, shots) must fit the 8 MiB (n <= 30 fits up to
+ *    65536 shots); larger requests return ALEPH_B200_INVALID_ARGUMENT.
+ *  - The first call on each device looks up the buffer's address (with that
+ *    device current) and should precede any stream capture.
+ *  - The buffer is shared by all handles on a device: calls that overlap in
+ *    time on one device (several host threads, or handles whose streams
+ *    run concurrently) race on it; serialise them. Each call synchronises
+ *    its handle's stream before it returns. */
+int aleph_b200_sample_cumulative_noalloc(aleph_b200_handle* h, aleph_b200_state* st, uint32_t shots,
+                                         const double* variates, uint64_t* out);
+
 /* ---- Backend::expectation_value (crates/aleph-sv/src/measure.rs:155-233) ---- */
 int aleph_b200_expectation(aleph_b200_handle* h, aleph_b200_state* st, const uint32_t* qubits,
                            const uint8_t* paulis, uint32_t n_terms, double coefficient, double* out);
