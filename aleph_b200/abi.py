@@ -143,6 +143,15 @@ class PassRecord(ct.Structure):
     ]
 
 
+class PlanConfig(ct.Structure):
+    _fields_ = [
+        ("precision", ct.c_int32),
+        ("tile_r", ct.c_uint32),
+        ("smem_max_n", ct.c_uint32),
+        ("block_window_search", ct.c_uint32),
+    ]
+
+
 PASS_KINDS = {1: "tile", 2: "smem", 3: "kq", 4: "measure", 5: "block", 6: "renorm"}
 
 # Every symbol include/aleph_b200.h declares, with its ctypes signature.
@@ -179,6 +188,9 @@ _SIGNATURES = {
     "aleph_b200_norm_sqr": ([_P, _P, ct.POINTER(ct.c_double)], ct.c_int),
     "aleph_b200_synchronize": ([_P], ct.c_int),
     "aleph_b200_get_stream": ([_P, ct.POINTER(_P)], ct.c_int),
+    "aleph_b200_describe_plan": (
+        [ct.c_uint32, ct.POINTER(PlanConfig), ct.POINTER(Instr), ct.c_uint64, ct.POINTER(Pools),
+         ct.POINTER(PassRecord), ct.c_uint64, ct.POINTER(ct.c_uint64)], ct.c_int),
     "aleph_b200_sample_cumulative_noalloc": (
         [_P, _P, ct.c_uint32, ct.POINTER(ct.c_double), ct.POINTER(ct.c_uint64)], ct.c_int),
     "aleph_b200_reset_state": ([_P, _P], ct.c_int),

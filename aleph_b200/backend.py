@@ -292,6 +292,24 @@ class CompiledPlan:
             pass
 
 
+def describe_plan(num_qubits: int, instructions, precision: str = "f64", tile_r: int = 5, smem_max_n: int = 12,
+                  block_window_search: bool = True) -> list[dict]:
+    """The passes the planner makes of ``instructions`` (host only, no device)."""
+    lib = abi.load_library()
+    flat = instructions if isinstance(instructions, Flat) else flatten(instructions)
+    cfg = abi.PlanConfig(abi.PRECISION[precision], tile_r, smem_max_n, int(bool(block_window_search)))
+    n = ct.c_uint64()
+    st = lib.aleph_b200_describe_plan(num_qubits, ct.byref(cfg), flat.instrs, flat.n, ct.byref(flat.pools), None, 0,
+                                      ct.byref(n))
+    if st != abi.OK:
+        raise _ERRORS.get(st, BackendError)(st, abi.STATUS_NAMES.get(st, str(st)))
+    buf = (abi.PassRecord * max(1, n.value))()
+    lib.aleph_b200_describe_plan(num_qubits, ct.byref(cfg), flat.instrs, flat.n, ct.byref(flat.pools), buf, n.value,
+                                 ct.byref(n))
+    return [{"kind": abi.PASS_KINDS.get(r.kind, r.kind), "gates": r.gates, "n": r.n, "qubits": list(r.qubits[: r.nq]),
+             "post_ops": r.post_ops, "bytes": r.bytes} for r in buf[: n.value]]
+
+
 def run_with_outcomes(backend: B200SvBackend, circuit: Circuit, measure_uniforms=None):
     """``run_with_outcomes`` (crates/aleph-backend/src/lib.rs:211-245)."""
     if circuit.num_qubits == 0 and len(circuit) == 0:

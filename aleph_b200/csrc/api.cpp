@@ -1046,12 +1046,51 @@ int aleph_b200_set_tuning(aleph_b200_handle* h, const char* key, int64_t value) 
     h->record_passes = value != 0;
     return ALEPH_B200_OK;
   }
+  if (!std::strcmp(key, "block_window_search")) {
+    h->opts.block_window_search = value != 0;
+    return ALEPH_B200_OK;
+  }
   if (!std::strcmp(key, "smem_max_n")) {
     if (value < 0 || value > 12) return set_error(h, ALEPH_B200_INVALID_ARGUMENT, "smem_max_n must be in 0..12");
     h->opts.smem_max_n = (uint32_t)value;
     return ALEPH_B200_OK;
   }
   return set_error(h, ALEPH_B200_INVALID_ARGUMENT, "unknown tuning key %s", key);
+}
+
+int aleph_b200_describe_plan(uint32_t num_qubits, const aleph_b200_plan_config* config, const aleph_b200_instr* in,
+                             uint64_t count, const aleph_b200_pools* pools, aleph_b200_pass_record* out, uint64_t cap,
+                             uint64_t* n_passes) {
+  if (!config || !n_passes || (!in && count) || (cap && !out)) return ALEPH_B200_INVALID_ARGUMENT;
+  if (config->precision < ALEPH_B200_F64 || config->precision > ALEPH_B200_TC32 || config->tile_r < 1 ||
+      config->tile_r > 5 || config->smem_max_n > 12 || num_qubits > 40)
+    return ALEPH_B200_INVALID_ARGUMENT;
+  FullHandle tmp;  // host-only: validation messages land here, no device is touched
+  tmp.opts.tile_r = config->tile_r;
+  tmp.opts.smem_max_n = config->smem_max_n;
+  tmp.opts.tensor_blocks = config->precision == ALEPH_B200_TC32;
+  tmp.opts.block_window_search = config->block_window_search != 0;
+  std::vector<Lowered> ops;
+  if (int r = lower_stream(&tmp, num_qubits, in, count, pools, &ops)) return r;
+  Plan P;
+  if (int s = build_plan(ops, num_qubits, tmp.opts, &P)) return s;
+  const double bpa = config->precision == ALEPH_B200_F64 ? 16.0 : 8.0;
+  const double len = (double)(1ull << num_qubits);
+  *n_passes = P.passes.size();
+  for (size_t k = 0; k < P.passes.size() && k < cap; ++k) {
+    const Pass& ps = P.passes[k];
+    aleph_b200_pass_record r{};
+    r.kind = (uint32_t)ps.kind;
+    r.gates = ps.gates;
+    r.n = num_qubits;
+    const uint32_t* qs = ps.kind == PASS_BLOCK ? ps.block.bq : ps.tile.hq;
+    r.nq = ps.kind == PASS_BLOCK ? 6 : ps.kind == PASS_TILE ? ps.tile.R : 0;
+    for (uint32_t j = 0; j < r.nq && j < 8; ++j) r.qubits[j] = qs[j];
+    r.post_ops = ps.kind == PASS_BLOCK ? ps.block.post_count : 0;
+    r.bytes = (ps.kind == PASS_MEASURE ? 3 : 2) * len * bpa;
+    out[k] = r;
+  }
+  return ALEPH_B200_OK;
 }
 
 int aleph_b200_get_pass_records(const aleph_b200_handle* h, aleph_b200_pass_record* out, uint64_t cap, uint64_t* n) {

@@ -119,6 +119,7 @@ struct PlanOptions {
   uint32_t smem_max_n = 12;     // states with n <= this run as one shared-memory pass
   bool tensor_blocks = false;   // TC32: fuse into 6-qubit dense blocks
   uint32_t block_k = 6;
+  bool block_window_search = true;  // TC32: also try every 6-qubit window per pass
 };
 
 // ---------------------------------------------------------------------------

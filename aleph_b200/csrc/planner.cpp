@@ -683,37 +683,69 @@ void apply_local(const Lowered& L, const uint32_t* bq, Cx* s) {
   }
 }
 
-int plan_segment_blocks(const std::vector<const Lowered*>& seg, uint32_t n, uint32_t R, Plan* P) {
+// One block pass drawn from the pending ops: the ops fused into the block
+// (`take`), the diagonal ops applied after it in the epilogue (`post`) and the
+// ops left for later passes (`rest`, in order). With `fixed`, the block
+// qubits are `fixedB`; otherwise they grow first-come up to 6 qubits. An op
+// joins only if it commutes past every op deferred before it.
+struct BlockTake {
+  uint64_t B = 0;
+  std::vector<const Lowered*> take, post, rest;
+  size_t score() const { return take.empty() ? 0 : take.size() + post.size(); }
+};
+
+void block_take(const std::vector<const Lowered*>& pending, uint64_t fixedB, bool fixed, BlockTake* out) {
+  uint64_t B = fixed ? fixedB : 0, bf = 0, bd = 0, post_lock = 0;
+  auto fits = [&](uint64_t supp) {
+    return fixed ? (supp & ~fixedB) == 0 : __builtin_popcountll(B | supp) <= 6;
+  };
+  for (const Lowered* L : pending) {
+    const uint64_t supp = L->nondiag | L->diag;
+    if (L->nondiag) {
+      if (!(L->nondiag & (bf | bd | post_lock)) && !(L->diag & bf) && fits(supp)) {
+        B |= supp;
+        out->take.push_back(L);
+        continue;
+      }
+    } else if (!(L->diag & bf)) {
+      if (fits(supp)) {
+        B |= supp;
+        out->take.push_back(L);
+        continue;
+      }
+      if (B != 0 && out->post.size() < 48) {  // the block kernel caches up to 48 post ops
+        out->post.push_back(L);
+        post_lock |= supp;
+        continue;
+      }
+    }
+    bf |= L->nondiag;
+    bd |= L->diag;
+    out->rest.push_back(L);
+  }
+  out->B = B;
+}
+
+int plan_segment_blocks(const std::vector<const Lowered*>& seg, uint32_t n, uint32_t R, bool window_search,
+                        Plan* P) {
   std::vector<const Lowered*> pending = seg;
   while (!pending.empty()) {
-    uint64_t B = 0, bf = 0, bd = 0, post_lock = 0;
-    std::vector<const Lowered*> take, post, rest;
-    for (const Lowered* L : pending) {
-      const uint64_t supp = L->nondiag | L->diag;
-      if (L->nondiag) {
-        const bool ok = !(L->nondiag & (bf | bd | post_lock)) && !(L->diag & bf) &&
-                        __builtin_popcountll(B | supp) <= 6;
-        if (ok) {
-          B |= supp;
-          take.push_back(L);
-          continue;
-        }
-      } else if (!(L->diag & bf)) {
-        if (__builtin_popcountll(B | supp) <= 6) {
-          B |= supp;
-          take.push_back(L);
-          continue;
-        }
-        if (B != 0 && post.size() < 48) {  // the block kernel caches up to 48 post ops
-          post.push_back(L);
-          post_lock |= supp;
-          continue;
-        }
+    // Candidates: the first-come block, and (window_search) every window of 6
+    // consecutive qubits; the one that consumes the most ops wins (ties keep
+    // the earlier candidate). On a brickwall the windows follow the light
+    // cone, which first-come growth does not.
+    BlockTake best;
+    block_take(pending, 0, false, &best);
+    if (window_search)
+      for (uint32_t a = 0; a + 6 <= n; ++a) {
+        BlockTake c;
+        block_take(pending, 0x3Full << a, true, &c);
+        if (c.score() > best.score()) best = std::move(c);
       }
-      bf |= L->nondiag;
-      bd |= L->diag;
-      rest.push_back(L);
-    }
+    uint64_t B = best.B;
+    std::vector<const Lowered*>& take = best.take;
+    std::vector<const Lowered*>& post = best.post;
+    std::vector<const Lowered*>& rest = best.rest;
     if (take.empty()) {
       // the head op does not fit a 6-qubit block: run it on the CUDA cores
       std::vector<const Lowered*> one{pending.front()};
@@ -781,7 +813,7 @@ int build_plan(const std::vector<Lowered>& ops, uint32_t n, const PlanOptions& o
     } else {
       // a 2-qubit gate may need two register qubits: R >= 2 unless only one high qubit exists
       const uint32_t R = std::min<uint32_t>(std::max<uint32_t>(o.tile_r, 2), std::min<uint32_t>(5, n - 5));
-      if (o.tensor_blocks && n >= 13) status = plan_segment_blocks(seg, n, R, P);
+      if (o.tensor_blocks && n >= 13) status = plan_segment_blocks(seg, n, R, o.block_window_search, P);
       else status = plan_segment_tiles(seg, n, R, P);
     }
     seg.clear();

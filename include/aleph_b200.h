@@ -300,6 +300,20 @@ typedef struct aleph_b200_pass_record {
   double ms;            /* device time of the pass (CUDA events on the handle's stream)    */
   double bytes;         /* algorithmic HBM bytes of the pass                               */
 } aleph_b200_pass_record;
+/* The passes the planner makes of a gate stream, without a device (ms = 0):
+ * what aleph_b200_compile would launch for a `num_qubits` register of the
+ * given precision and tuning. For plan inspection, the autotuner and the
+ * learned planner's features. Returns the validation error of the first
+ * invalid record, like aleph_b200_compile. */
+typedef struct aleph_b200_plan_config {
+  int32_t precision;             /* aleph_b200_precision                     */
+  uint32_t tile_r;               /* register qubits per warp tile (1..5)     */
+  uint32_t smem_max_n;           /* n <= this: one shared-memory pass        */
+  uint32_t block_window_search;  /* TC32: also try every 6-qubit window      */
+} aleph_b200_plan_config;
+int aleph_b200_describe_plan(uint32_t num_qubits, const aleph_b200_plan_config* config, const aleph_b200_instr* instrs,
+                             uint64_t count, const aleph_b200_pools* pools, aleph_b200_pass_record* out, uint64_t cap,
+                             uint64_t* n_passes);
 /* Records of the last gate stream run with "record_passes" on; *n = count. */
 int aleph_b200_get_pass_records(const aleph_b200_handle* h, aleph_b200_pass_record* out, uint64_t cap,
                                 uint64_t* n);

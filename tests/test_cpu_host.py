@@ -169,3 +169,28 @@ def test_oracle_errors():
     with pytest.raises(oracle.OracleError) as e:
         oracle.run(2, [C.Reset(0)])
     assert e.value.status == abi.UNSUPPORTED_INSTRUCTION
+
+
+# ---- planner (host only) -------------------------------------------------------
+def test_describe_plan_counts_passes_without_a_device():
+    from aleph_b200.backend import describe_plan
+
+    c = workloads.brickwall(32, 40, seed=0)
+    greedy = describe_plan(32, c.instructions, "tc32", block_window_search=False)
+    search = describe_plan(32, c.instructions, "tc32", block_window_search=True)
+    assert all(p["kind"] == "block" for p in search)
+    # every gate lands in exactly one pass
+    assert sum(p["gates"] for p in search) == sum(p["gates"] for p in greedy) == c.gate_count()
+    # the 6-qubit window search follows the brickwall light cone: far fewer passes
+    assert len(search) <= 72 < len(greedy)
+    f64 = describe_plan(32, c.instructions, "f64")
+    assert all(p["kind"] == "tile" for p in f64) and sum(p["gates"] for p in f64) == c.gate_count()
+    assert all(p["bytes"] == 2 * 16 * 2.0**32 for p in f64)
+
+
+def test_describe_plan_reports_validation_errors():
+    from aleph_b200.backend import BackendError, describe_plan
+
+    with pytest.raises(BackendError) as e:
+        describe_plan(4, [C.GateInstance(C.H(), [4])])
+    assert e.value.status == abi.QUBIT_OUT_OF_RANGE

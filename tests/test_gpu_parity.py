@@ -363,3 +363,13 @@ def test_compiled_plan_matches_stream(precision):
     with pytest.raises(Exception):
         plan.execute(st, [0.5])
     plan.free()
+
+
+@pytest.mark.parametrize("window_search", [0, 1])
+def test_tc32_block_planners(window_search):
+    n = 17
+    c = workloads.brickwall(n, 12, seed=51)
+    got, _, be, _ = engine_state(c, precision="tc32", block_window_search=window_search)
+    want, _ = oracle.run(n, c.instructions)
+    assert np.abs(got - want).max() <= TC_TOL
+    assert 1.0 - fidelity(got, want) <= 1e-6
