@@ -14,8 +14,9 @@
 //   `target < cumulative`, zero bins skipped, last positive bin as fallback.
 //   Shots are resolved in parallel on a two-level prefix (tree block sums +
 //   a sequential scan inside the block); a shot whose target lies within the
-//   rounding bound of a bin boundary is re-resolved by an exact sequential
-//   scan (for n <= 26), so the outcome equals the sequential CPU result.
+//   rounding bound of a bin boundary is re-resolved against the exact
+//   sequential running sum (for n <= 28), so the outcome equals the
+//   sequential CPU result.
 
 #include <cmath>
 
@@ -24,7 +25,7 @@
 namespace ab {
 
 constexpr uint32_t CUM_BLOCK = 2048;  // amplitudes per level-1 CDF block
-constexpr uint32_t EXACT_MAX_N = 26;  // exact re-resolution of ambiguous shots up to this n
+constexpr uint32_t EXACT_MAX_N = 28;  // exact re-resolution of ambiguous shots up to this n
 
 template <typename Real>
 __device__ __forceinline__ double prob_exact(const V2<Real>* amps, uint64_t i) {
@@ -138,39 +139,116 @@ __global__ void alias_partition_kernel(uint64_t len, AliasScratch s) {
   }
 }
 
-// The Vose loop of AliasTable::build with both stacks' tops tracked exactly.
-// status[0] is set on failure (never expected: the loop is bounded by N).
-__global__ void alias_chain_kernel(uint64_t len, AliasScratch s, int32_t* status) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+// The Vose loop of AliasTable::build, one warp.
+//
+// With LIFO stacks, the element pushed in one step is popped in the next: a
+// large whose residual stays >= 1 is the next large, one that drops below 1
+// is the next small. So that element lives in lane 0's registers, and the
+// stacks themselves are only ever popped: their entries below the top, and
+// the scaled values of those entries, are read-only until popped. The warp
+// therefore streams them into shared-memory buffers ahead of the chain
+// (descending stack order), and lane 0 runs the dependent chain out of
+// shared memory with the reference's operation order,
+//   alias[s] = l, threshold[s] = value(s), value(l) = (value(l) + value(s)) - 1.
+// status[0] is set on failure (never expected: the loop is bounded by 2N).
+constexpr int CHAIN_CH = 1024;
+__global__ void __launch_bounds__(32) alias_chain_kernel(uint64_t len, AliasScratch s, int32_t* status) {
+  __shared__ uint32_t sbi[CHAIN_CH], lbi[CHAIN_CH];
+  __shared__ double sbv[CHAIN_CH], lbv[CHAIN_CH];
+  const int lane = threadIdx.x;
   if (len == 1) {
-    s.prob[0] = 1.0;
-    s.alias[0] = 0;
+    if (lane == 0) {
+      s.prob[0] = 1.0;
+      s.alias[0] = 0;
+    }
     return;
   }
-  int64_t ts = (int64_t)s.totals[0];  // small stack height (stack = small[0..ts))
-  int64_t tl = (int64_t)s.totals[1];  // large stack height
-  uint32_t* SS = s.small;
-  uint32_t* LS = s.large;
+  int64_t ts = (int64_t)s.totals[0];  // small entries not yet buffered: small[0..ts)
+  int64_t tl = (int64_t)s.totals[1];  // large entries not yet buffered: large[0..tl)
+  int ns = 0, ps = 0, nl = 0, pl = 0;  // buffer fill / consumed counts (uniform over the warp)
+  bool hs = false, hl = false;         // lane 0: current small / large held in registers
+  uint32_t si = 0, li = 0;
+  double sv = 0.0, lv = 0.0;
   uint64_t guard = 0;
-  while (ts > 0 && tl > 0) {
-    if (++guard > 2 * len + 4) {
+  int fail = 0;
+  while (true) {
+    if (ps == ns && ts > 0) {  // refill the small buffer from the stack top
+      const int m = ts < CHAIN_CH ? (int)ts : CHAIN_CH;
+      for (int k = lane; k < m; k += 32) {
+        const uint32_t id = s.small[ts - 1 - k];
+        sbi[k] = id;
+        sbv[k] = s.prob[id];
+      }
+      ts -= m;
+      ns = m;
+      ps = 0;
+    }
+    if (pl == nl && tl > 0) {
+      const int m = tl < CHAIN_CH ? (int)tl : CHAIN_CH;
+      for (int k = lane; k < m; k += 32) {
+        const uint32_t id = s.large[tl - 1 - k];
+        lbi[k] = id;
+        lbv[k] = s.prob[id];
+      }
+      tl -= m;
+      nl = m;
+      pl = 0;
+    }
+    __syncwarp();
+    int done = 0;
+    if (lane == 0) {
+      while (true) {
+        if (!hs && ps < ns) {
+          si = sbi[ps];
+          sv = sbv[ps];
+          ++ps;
+          hs = true;
+        }
+        if (!hl && pl < nl) {
+          li = lbi[pl];
+          lv = lbv[pl];
+          ++pl;
+          hl = true;
+        }
+        if (!hs || !hl) break;
+        if (++guard > 2 * len + 4) {
+          fail = 1;
+          break;
+        }
+        s.alias[si] = li;
+        s.prob[si] = sv;  // threshold = value of the small
+        const double r = __dsub_rn(__dadd_rn(lv, sv), 1.0);
+        if (r < 1.0) {  // the large becomes the next small
+          si = li;
+          sv = r;
+          hl = false;
+        } else {
+          lv = r;
+          hs = false;
+        }
+      }
+      done = fail || (!hs && ps == ns && ts == 0) || (!hl && pl == nl && tl == 0);
+    }
+    ps = __shfl_sync(0xffffffffu, ps, 0);
+    pl = __shfl_sync(0xffffffffu, pl, 0);
+    done = __shfl_sync(0xffffffffu, done, 0);
+    __syncwarp();
+    if (done) break;
+  }
+  if (lane == 0) {
+    if (fail) {
       status[0] = ALEPH_B200_DEVICE_FAILURE;
       return;
     }
-    const uint32_t sidx = SS[--ts];
-    const uint32_t lidx = LS[--tl];
-    const double ss = s.prob[sidx];
-    const double sl = s.prob[lidx];
-    s.prob[sidx] = ss;  // threshold = scaled[s]
-    s.alias[sidx] = lidx;
-    const double nl = __dsub_rn(__dadd_rn(sl, ss), 1.0);
-    s.prob[lidx] = nl;
-    if (nl < 1.0) SS[ts++] = lidx;
-    else LS[tl++] = lidx;
+    // Leftovers, drained below as self-aliases with threshold 1: the stack
+    // entries never popped (still in memory below the buffered ones) plus the
+    // element held in registers, pushed back on its stack.
+    int64_t rs = ts + (ns - ps), rl = tl + (nl - pl);
+    if (hs) s.small[rs++] = si;
+    if (hl) s.large[rl++] = li;
+    s.totals[0] = (uint32_t)rs;
+    s.totals[1] = (uint32_t)rl;
   }
-  // leftovers: self-alias with threshold 1 (drained by a parallel kernel below)
-  s.totals[0] = (uint32_t)ts;
-  s.totals[1] = (uint32_t)tl;
 }
 
 __global__ void alias_drain_kernel(AliasScratch s) {
@@ -206,6 +284,8 @@ struct CumScratch {
   double* norm;      // 2: [total, non-finite count]
   uint32_t* namb;    // ambiguous shot count
   uint32_t* amb;     // shots: ambiguous shot ids
+  double* ck;        // exact mode: sequential sum at the end of every SEQ_CH chunk
+  double* seq;       // exact mode: [sequential total, last positive index (bits)]
 };
 
 template <typename Real>
@@ -238,16 +318,36 @@ __global__ void cum_blocks_kernel(const V2<Real>* __restrict__ amps, uint64_t le
   }
 }
 
-__global__ void cum_prefix_kernel(CumScratch c, uint32_t nb) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  double run = 0.0;
-  for (uint32_t b = 0; b < nb; ++b) {
+// Exclusive prefix of the block sums, one CTA of PREFIX_T threads: thread t
+// sums a contiguous range, the range totals are scanned in shared memory, and
+// each thread writes its range's prefixes. The draws treat this prefix as an
+// approximation (guard band E below), so its rounding order is free.
+constexpr uint32_t PREFIX_T = 1024;
+__global__ void __launch_bounds__(PREFIX_T) cum_prefix_kernel(CumScratch c, uint32_t nb) {
+  __shared__ double part[PREFIX_T];
+  const uint32_t t = threadIdx.x;
+  const uint32_t per = (nb + PREFIX_T - 1) / PREFIX_T;
+  const uint32_t b0 = min(nb, t * per), b1 = min(nb, b0 + per);
+  double s = 0.0;
+  for (uint32_t b = b0; b < b1; ++b) s += c.bsum[b];
+  part[t] = s;
+  __syncthreads();
+  for (uint32_t off = 1; off < PREFIX_T; off <<= 1) {  // inclusive Hillis-Steele scan
+    const double v = t >= off ? part[t - off] : 0.0;
+    __syncthreads();
+    part[t] += v;
+    __syncthreads();
+  }
+  double run = t ? part[t - 1] : 0.0;
+  for (uint32_t b = b0; b < b1; ++b) {
     const double x = c.bsum[b];
     c.bsum[b] = run;
     run += x;
   }
-  c.bsum[nb] = run;
-  c.norm[0] = run;
+  if (t == PREFIX_T - 1) {
+    c.bsum[nb] = part[PREFIX_T - 1];
+    c.norm[0] = part[PREFIX_T - 1];
+  }
 }
 
 template <typename Real>
@@ -295,40 +395,95 @@ __global__ void cum_draw_kernel(const V2<Real>* __restrict__ amps, uint64_t len,
   }
 }
 
-// Exact sequential resolution of the ambiguous shots: the reference's
-// validate_norm total and cumulative_index scan, element by element.
+// Exact resolution of the ambiguous shots, in two kernels.
+//
+// cum_seq_kernel: the reference's sequential left-to-right sum
+// (validate_norm's total and cumulative_index's running sum are the same
+// sequence S_i = fl(S_{i-1} + p_i)), done once by one thread while the rest
+// of the CTA stages the next chunk of probabilities in shared memory. It
+// records S at the end of every SEQ_CH-element chunk (exact checkpoints),
+// the total and the last positive index.
+// cum_exact_kernel: per ambiguous shot, the first chunk whose checkpoint
+// exceeds the target, rescanned sequentially from the previous checkpoint,
+// so every outcome equals the sequential CPU scan's.
+constexpr uint32_t SEQ_CH = 2048;
+constexpr uint32_t SEQ_T = 512;
+
+template <typename Real>
+__global__ void __launch_bounds__(SEQ_T) cum_seq_kernel(const V2<Real>* __restrict__ amps, uint64_t len, CumScratch c) {
+  __shared__ double buf[2][SEQ_CH];
+  if (*c.namb == 0) return;  // uniform over the CTA: no ambiguous shot, nothing to resolve
+  const uint64_t nch = (len + SEQ_CH - 1) / SEQ_CH;
+  auto stage = [&](uint64_t ch, int slot) {
+    const uint64_t b0 = ch * SEQ_CH;
+    for (uint32_t j = threadIdx.x; j < SEQ_CH; j += SEQ_T)
+      buf[slot][j] = b0 + j < len ? prob_exact<Real>(amps, b0 + j) : 0.0;
+  };
+  stage(0, 0);
+  __syncthreads();
+  double S = 0.0;
+  int64_t last_pos = -1;
+  for (uint64_t ch = 0; ch < nch; ++ch) {
+    if (threadIdx.x == 0) {
+      const double* b = buf[ch & 1];
+      const uint64_t left = len - ch * SEQ_CH;
+      const uint32_t m = left < SEQ_CH ? (uint32_t)left : SEQ_CH;
+#pragma unroll 16
+      for (uint32_t j = 0; j < m; ++j) {
+        const double p = b[j];
+        S += p;
+        if (p > 0.0) last_pos = (int64_t)(ch * SEQ_CH + j);
+      }
+      c.ck[ch] = S;
+    } else if (ch + 1 < nch) {
+      // threads 1.. stage the next chunk (thread 0's share falls to the others)
+      const uint64_t b0 = (ch + 1) * SEQ_CH;
+      for (uint32_t j = threadIdx.x - 1; j < SEQ_CH; j += SEQ_T - 1)
+        buf[(ch + 1) & 1][j] = b0 + j < len ? prob_exact<Real>(amps, b0 + j) : 0.0;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    c.seq[0] = S;
+    c.seq[1] = __longlong_as_double(last_pos);
+  }
+}
+
 template <typename Real>
 __global__ void cum_exact_kernel(const V2<Real>* __restrict__ amps, uint64_t len, CumScratch c,
                                  const double* __restrict__ uniforms, uint64_t* __restrict__ out, int32_t* status) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
   const uint32_t na = *c.namb;
-  if (na == 0) return;
-  double total = 0.0;
-  for (uint64_t i = 0; i < len; ++i) total += prob_exact<Real>(amps, i);
-  // insertion-sort the ambiguous shots by target (they are few)
-  uint32_t* ids = c.amb;
-  for (uint32_t a = 1; a < na; ++a)
-    for (uint32_t b = a; b > 0 && uniforms[ids[b - 1]] > uniforms[ids[b]]; --b) {
-      const uint32_t t = ids[b];
-      ids[b] = ids[b - 1];
-      ids[b - 1] = t;
+  const uint64_t nch = (len + SEQ_CH - 1) / SEQ_CH;
+  const double total = c.seq[0];
+  const int64_t last_pos = __double_as_longlong(c.seq[1]);
+  for (uint32_t a = blockIdx.x * blockDim.x + threadIdx.x; a < na; a += gridDim.x * blockDim.x) {
+    const uint32_t k = c.amb[a];
+    const double target = uniforms[k] * total;
+    // first chunk whose inclusive checkpoint exceeds the target
+    uint64_t lo = 0, hi = nch;
+    while (lo < hi) {
+      const uint64_t mid = (lo + hi) >> 1;
+      if (target < c.ck[mid]) hi = mid;
+      else lo = mid + 1;
     }
-  uint32_t next = 0;
-  double cum = 0.0;
-  int64_t last_pos = -1;
-  for (uint64_t i = 0; i < len && next < na; ++i) {
-    const double p = prob_exact<Real>(amps, i);
-    if (p > 0.0) {
-      last_pos = (int64_t)i;
-      cum += p;
-      while (next < na && uniforms[ids[next]] * total < cum) out[ids[next++]] = i;
+    if (lo == nch) {  // target >= total: the last positive bin
+      if (last_pos < 0) status[0] = ALEPH_B200_INVALID_STATE;
+      else out[k] = (uint64_t)last_pos;
+      continue;
+    }
+    double S = lo ? c.ck[lo - 1] : 0.0;
+    const uint64_t e = (lo + 1) * SEQ_CH < len ? (lo + 1) * SEQ_CH : len;
+    for (uint64_t i = lo * SEQ_CH; i < e; ++i) {
+      const double p = prob_exact<Real>(amps, i);
+      if (p > 0.0) {
+        S += p;
+        if (target < S) {
+          out[k] = i;
+          break;
+        }
+      }
     }
   }
-  if (last_pos < 0) {
-    status[0] = ALEPH_B200_INVALID_STATE;
-    return;
-  }
-  while (next < na) out[ids[next++]] = (uint64_t)last_pos;
 }
 
 size_t sample_scratch_bytes(uint32_t n, int mode, uint32_t shots) {
@@ -338,7 +493,8 @@ size_t sample_scratch_bytes(uint32_t n, int mode, uint32_t shots) {
     return len * (8 + 4 + 4 + 4) + nb * (8 + 16) + 256;
   }
   const uint64_t nb = (len + CUM_BLOCK - 1) / CUM_BLOCK;
-  return (nb + 1) * 8 + 64 + 256 + (size_t)shots * 4;
+  const uint64_t nch = n <= EXACT_MAX_N ? (len + SEQ_CH - 1) / SEQ_CH : 0;  // exact-mode checkpoints
+  return (nb + 1) * 8 + 64 + 256 + (size_t)shots * 4 + 16 + nch * 8 + 32;
 }
 
 static inline char* align_up(char* p, size_t a) {
@@ -383,11 +539,14 @@ cudaError_t launch_sample(const void* amps, int precision, uint32_t n, uint32_t 
   c.namb = (uint32_t*)p; p += 16;
   c.amb = (uint32_t*)align_up(p, 16);
   p = (char*)(c.amb + shots);
+  const uint64_t nch = n <= EXACT_MAX_N ? (len + SEQ_CH - 1) / SEQ_CH : 0;
+  c.seq = (double*)align_up(p, 16); p = (char*)(c.seq + 2);
+  c.ck = (double*)p; p += nch * 8;
   if ((size_t)(p - (char*)scratch) > scratch_bytes) return cudaErrorInvalidValue;
   cudaMemsetAsync(c.norm, 0, 32, st);
   if (f64) cum_blocks_kernel<double><<<nb, 256, 0, st>>>((const double2*)amps, len, c);
   else cum_blocks_kernel<float><<<nb, 256, 0, st>>>((const float2*)amps, len, c);
-  cum_prefix_kernel<<<1, 32, 0, st>>>(c, nb);
+  cum_prefix_kernel<<<1, PREFIX_T, 0, st>>>(c, nb);
   check_norm_kernel<<<1, 32, 0, st>>>(c.norm, norm_tolerance(len, precision), status);
   if (shots) {
     if (f64)
@@ -397,8 +556,14 @@ cudaError_t launch_sample(const void* amps, int precision, uint32_t n, uint32_t 
       cum_draw_kernel<float><<<(shots + 127) / 128, 128, 0, st>>>((const float2*)amps, len, nb, c,
                                                                   (const double*)variates, shots, out, status);
     if (n <= EXACT_MAX_N) {
-      if (f64) cum_exact_kernel<double><<<1, 32, 0, st>>>((const double2*)amps, len, c, (const double*)variates, out, status);
-      else cum_exact_kernel<float><<<1, 32, 0, st>>>((const float2*)amps, len, c, (const double*)variates, out, status);
+      const unsigned eb = (shots + 127) / 128;
+      if (f64) {
+        cum_seq_kernel<double><<<1, SEQ_T, 0, st>>>((const double2*)amps, len, c);
+        cum_exact_kernel<double><<<eb, 128, 0, st>>>((const double2*)amps, len, c, (const double*)variates, out, status);
+      } else {
+        cum_seq_kernel<float><<<1, SEQ_T, 0, st>>>((const float2*)amps, len, c);
+        cum_exact_kernel<float><<<eb, 128, 0, st>>>((const float2*)amps, len, c, (const double*)variates, out, status);
+      }
     }
   }
   return cudaGetLastError();

@@ -155,7 +155,7 @@ def test_mid_circuit_measurement(n):
     assert np.abs(got - want).max() <= F64_TOL
 
 
-@pytest.mark.parametrize("n", [1, 5, 12, 18])
+@pytest.mark.parametrize("n", [1, 5, 12, 18, 22])
 def test_sampling_alias_identical(n):
     c = workloads.brickwall(n, 6, seed=10) if n > 1 else C.Circuit(1).add(C.Ry(1.1), [0])
     be = B200SvBackend(seed=0)
@@ -166,7 +166,7 @@ def test_sampling_alias_identical(n):
     assert np.array_equal(shots, oracle.sample_alias(psi, words))
 
 
-@pytest.mark.parametrize("n", [1, 6, 12, 16])
+@pytest.mark.parametrize("n", [1, 6, 12, 16, 22, 24])
 def test_sampling_cumulative_identical(n):
     c = workloads.brickwall(n, 6, seed=11) if n > 1 else C.Circuit(1).add(C.Ry(0.7), [0])
     be = B200SvBackend(seed=0)
