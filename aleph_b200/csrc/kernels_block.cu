@@ -13,27 +13,33 @@
 // accumulated in FP32 in TMEM: ~16 significant bits per operand at three BF16
 // MMAs per product.
 //
-// Warp-specialised persistent kernel, one CTA per SM, 10 warps:
-//   * warp 8 (TMA): fetches each tile (64 block rows x 128 columns = 64 KiB
+// Warp-specialised persistent kernel, one CTA per SM, 18 warps:
+//   * warp 16 (TMA): fetches each tile (64 block rows x 128 columns = 64 KiB
 //     FP32) with plain (non-multicast) cp.async.bulk copies of its contiguous
 //     runs into one of two shared-memory stages (mbarrier transaction counts);
-//   * warps 0-3 (converters): thread c takes column c of the staged tile,
-//     splits its 128 real values into BF16 hi/lo and writes them with
-//     tcgen05.st into TMEM lane c — the A operand of the MMA lives in tensor
-//     memory (two buffers), so shared memory only holds W and the stages;
-//   * warp 9 (one thread): issues 3 x 8 tcgen05.mma (A from TMEM, M=128
+//   * warps 0-7 (converters): thread c takes column c of the staged tile (one
+//     half of its block rows per warp group), splits the real values into
+//     BF16 hi/lo and writes them with tcgen05.st into TMEM lane c: the A
+//     operand of the MMA lives in tensor memory (two buffers), so shared
+//     memory only holds W and the stages;
+//   * warp 17 (one thread): issues 3 x 8 tcgen05.mma (A from TMEM, M=128
 //     columns; B = W_hi / W_lo from shared memory, N=128, K=16; kind::f16,
 //     BF16 in, FP32 accumulate) into one of two TMEM accumulators and commits
 //     to mbarriers that free the A buffer and hand the accumulator over;
-//   * warps 4-7 (epilogue): tcgen05.ld the accumulator (32x32b: one column per
-//     thread, real and imaginary parts of all 64 outputs), apply the diagonal
-//     ops that follow the block (CZ-like sign flips as one 64-bit row mask per
-//     thread, other phases per element) and store straight to HBM.
+//   * warps 8-15 (epilogue): tcgen05.ld the accumulator (32x32b: one column
+//     per thread), apply the diagonal ops that follow the block (CZ-like sign
+//     flips as one 64-bit row mask per thread, other phases per element) and
+//     store straight to HBM (16-byte stores of row pairs when the block holds
+//     qubit 0, whose rows are then adjacent).
 // TMEM: accumulators D0, D1 at columns 0 / 128, A0, A1 at 256 / 384 (hi in the
 // first 64 columns, lo in the next 64): all 512 columns.
-// Loads of tile t+2, splits of t+1 and MMAs/stores of t overlap. Every wait
-// is bounded; on expiry the CTA records an error code, every role leaves its
-// loop, the TMEM is freed and the kernel returns.
+// Stage layout: the tile's contiguous runs back to back, each followed by a
+// pad chosen on the host so that the 32 columns a warp touches at one block
+// row fall in distinct shared-memory banks (for blocks on low qubits, whose
+// columns are far apart within a run, the columns are chosen above a gap so
+// that they index runs, and the pad skews the runs).
+// Every wait is bounded; on expiry the CTA records an error code, every role
+// leaves its loop, the TMEM is freed and the kernel returns.
 
 #include <cstdint>
 #include <cstring>
@@ -55,6 +61,9 @@ constexpr int ROLE_WARPS = 8;   // converter / epilogue warps (mbarrier arrival 
 constexpr int NCOL = 128;                     // columns per tile (MMA M)
 constexpr int TILE_AMPS = 64 * NCOL;          // 8192 complex
 constexpr int TILE_BYTES = TILE_AMPS * 8;     // 64 KiB FP32 complex
+constexpr int MAX_PAD_BYTES = 4096;           // run padding per stage (bank-conflict skew)
+constexpr int STAGE_BYTES = TILE_BYTES + MAX_PAD_BYTES;
+constexpr int MAX_RUNS = 128;                 // runs per tile (contiguous prefix >= 6 qubits)
 constexpr int W_BYTES = 2 * 128 * 128 * 2;    // hi + lo images, 64 KiB
 constexpr uint32_t TMEM_COLS = 512;
 constexpr uint32_t TM_D = 0, TM_A = 256;      // accumulators / A operands (128 columns each)
@@ -64,8 +73,8 @@ constexpr int MAX_POST = 48;
 // shared-memory map (offsets from a 1024-byte aligned base)
 constexpr int OFF_W = 0;                                  // B operand: W_hi | W_lo
 constexpr int OFF_S = OFF_W + W_BYTES;                    // two FP32 input stages
-constexpr int OFF_TAB = OFF_S + 2 * TILE_BYTES;           // index tables
-constexpr int TAB_BYTES = 64 * 4 + NCOL * 4 + 64 * 8 + 64 * 8 + NCOL * 8;
+constexpr int OFF_TAB = OFF_S + 2 * STAGE_BYTES;          // lane-indexed tables
+constexpr int TAB_BYTES = NCOL * 4 + NCOL * 8 + MAX_RUNS * 8;
 constexpr int OFF_BAR = OFF_TAB + TAB_BYTES;              // mbarriers
 constexpr int SMEM_BYTES = OFF_BAR + 128 + 1024;          // + alignment slack
 
@@ -204,11 +213,17 @@ struct BlockArgs {
   int* err;
   uint32_t n;
   uint32_t bq[6];
-  // Per block row j: tile-local index and global offset. Kept in the
+  uint64_t tmask;                       // tile qubits: block + column qubits
+  uint32_t nruns, run_bytes, run_stride;  // contiguous runs of a tile; stage bytes between runs
+  // Per block row j: byte offset in a stage and global offset. Kept in the
   // kernel-parameter (constant) bank so the unrolled per-element loops of the
   // converters and the epilogue read them as instruction operands.
-  uint32_t lrow[64];
+  uint32_t rowoff[64];
   uint64_t grow[64];
+  // Lane-indexed tables, copied to shared memory by the kernel.
+  uint32_t coloff[128];  // byte offset of column c in a stage
+  uint64_t gcol[128];    // global offset of column c
+  uint64_t runoff[128];  // global offset of run r
 };
 
 __global__ void __launch_bounds__(blk::THREADS, 1) block_kernel(const __grid_constant__ BlockArgs a) {
@@ -216,14 +231,12 @@ __global__ void __launch_bounds__(blk::THREADS, 1) block_kernel(const __grid_con
   extern __shared__ uint8_t smem_raw[];
   uint8_t* sm = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   const uint32_t sbase = smem_u32(sm);
-  uint32_t* Lrow = (uint32_t*)(sm + OFF_TAB);  // tile-local index of block row j
-  uint32_t* Lcol = Lrow + 64;                  // tile-local index of column c
-  uint64_t* runoff = (uint64_t*)(Lcol + NCOL); // global offset of run r
-  uint64_t* Grow = runoff + 64;                // global offset of block row j
-  uint64_t* Gcol = Grow + 64;                  // global offset of column c
+  uint32_t* Lcol = (uint32_t*)(sm + OFF_TAB);   // stage byte offset of column c
+  uint64_t* Gcol = (uint64_t*)(Lcol + NCOL);    // global offset of column c
+  uint64_t* runoff = Gcol + NCOL;               // global offset of run r
   const uint32_t bar_w = sbase + OFF_BAR;
-  const uint32_t bar_sfull = bar_w + 8;         // [2] TMA -> converters
-  const uint32_t bar_sempty = bar_sfull + 16;   // [2] converters -> TMA
+  const uint32_t bar_sfull = bar_w + 8;         // [2] TMA -> converters: tile loaded
+  const uint32_t bar_sempty = bar_sfull + 16;   // [2] converters -> TMA: stage read
   const uint32_t bar_afull = bar_sempty + 16;   // [2] converters -> MMA
   const uint32_t bar_aempty = bar_afull + 16;   // [2] MMA -> converters
   const uint32_t bar_dfull = bar_aempty + 16;   // [2] MMA -> epilogue
@@ -238,56 +251,15 @@ __global__ void __launch_bounds__(blk::THREADS, 1) block_kernel(const __grid_con
   const uint32_t n = a.n;
   volatile int* abort_flag = &abort_sh;
 
-  // ---- tile geometry -------------------------------------------------------
-  // Tile qubit set T = block qubits + the 7 lowest other qubits (the column
-  // bits). T contains all qubits 0..c-1 (one contiguous run of 2^c
-  // amplitudes) plus the block qubits above them; tile-local index bits
-  // follow T in ascending order.
+  // ---- tile geometry (computed on the host) ---------------------------------
   uint64_t bmask = 0;
   for (int j = 0; j < 6; ++j) bmask |= 1ull << a.bq[j];
-  uint32_t cols[7];
-  {
-    int k = 0;
-    for (uint32_t q = 0; q < n && k < 7; ++q)
-      if (!((bmask >> q) & 1)) cols[k++] = q;
-  }
-  uint64_t tmask = bmask;
-  for (int k = 0; k < 7; ++k) tmask |= 1ull << cols[k];
-  uint32_t c = 0;
-  while (c < 13 && ((tmask >> c) & 1)) ++c;  // contiguous run: qubits 0..c-1
-  const uint32_t nruns = 1u << (13 - c), run_bytes = (1u << c) * 8;
-  auto local_pos = [&](uint32_t q) -> uint32_t { return (uint32_t)__popcll(tmask & ((1ull << q) - 1)); };
+  const uint64_t tmask = a.tmask;
+  const uint32_t nruns = a.nruns, run_bytes = a.run_bytes, run_stride = a.run_stride;
   if (tid < NCOL) {
-    uint32_t lc = 0;
-    uint64_t gc = 0;
-    for (int k = 0; k < 7; ++k)
-      if ((tid >> k) & 1) {
-        lc |= 1u << local_pos(cols[k]);
-        gc |= 1ull << cols[k];
-      }
-    Lcol[tid] = lc;
-    Gcol[tid] = gc;
-  }
-  if (tid < 64) {
-    uint32_t lr = 0;
-    uint64_t gr = 0;
-    for (int j = 0; j < 6; ++j)
-      if ((tid >> j) & 1) {
-        lr |= 1u << local_pos(a.bq[j]);
-        gr |= 1ull << a.bq[j];
-      }
-    Lrow[tid] = lr;
-    Grow[tid] = gr;
-    uint64_t off = 0;  // run r: local bits c..12 -> the T qubits above c-1
-    if ((uint32_t)tid < nruns) {
-      uint32_t bit = 0;
-      for (uint32_t q = c; q < n; ++q)
-        if ((tmask >> q) & 1) {
-          if ((tid >> bit) & 1) off |= 1ull << q;
-          ++bit;
-        }
-    }
-    runoff[tid] = off;
+    Lcol[tid] = a.coloff[tid];
+    Gcol[tid] = a.gcol[tid];
+    runoff[tid] = a.runoff[tid];
   }
   if (tid == 0) {
     mbar_init(bar_w, 1);
@@ -360,9 +332,9 @@ __global__ void __launch_bounds__(blk::THREADS, 1) block_kernel(const __grid_con
       const uint64_t base = tile_base(t);
       if (lane == 0) mbar_expect_tx(bar_sfull + 8 * s, TILE_BYTES);
       __syncwarp();
-      const uint32_t dst0 = sbase + OFF_S + s * TILE_BYTES;
+      const uint32_t dst0 = sbase + OFF_S + s * STAGE_BYTES;
       for (uint32_t r = lane; r < nruns; r += 32)
-        bulk_load(dst0 + r * run_bytes, a.amps + (base | runoff[r]), run_bytes, bar_sfull + 8 * s);
+        bulk_load(dst0 + r * run_stride, a.amps + (base | runoff[r]), run_bytes, bar_sfull + 8 * s);
     }
   } else if (warp < EPI_WARP0) {
     // ---------------- converters: stage -> BF16 hi/lo -> TMEM A operand ----------------
@@ -378,16 +350,16 @@ __global__ void __launch_bounds__(blk::THREADS, 1) block_kernel(const __grid_con
         break;
       }
       tc_fence_after();
-      const float2* stg = (const float2*)(sm + OFF_S + s * TILE_BYTES);
+      const uint8_t* stg = sm + OFF_S + s * STAGE_BYTES + lc;  // this thread's column
       const uint32_t ta = tmem + TM_A + 128 * s + ((uint32_t)(32 * q) << 16);  // this warp's lanes
       {
         uint32_t hr[16], hi[16], lr[16], li[16];
 #pragma unroll
         for (int p = 0; p < 16; ++p) {
-          const uint32_t r0 = h ? a.lrow[32 + 2 * p] : a.lrow[2 * p];
-          const uint32_t r1 = h ? a.lrow[33 + 2 * p] : a.lrow[2 * p + 1];
-          const float2 x0 = stg[r0 | lc];
-          const float2 x1 = stg[r1 | lc];
+          const uint32_t r0 = h ? a.rowoff[32 + 2 * p] : a.rowoff[2 * p];
+          const uint32_t r1 = h ? a.rowoff[33 + 2 * p] : a.rowoff[2 * p + 1];
+          const float2 x0 = *(const float2*)(stg + r0);
+          const float2 x1 = *(const float2*)(stg + r1);
           const uint32_t a0 = bf16_bits(x0.x), a1 = bf16_bits(x1.x);
           const uint32_t b0 = bf16_bits(x0.y), b1 = bf16_bits(x1.y);
           hr[p] = a0 | (a1 << 16);
@@ -438,9 +410,12 @@ __global__ void __launch_bounds__(blk::THREADS, 1) block_kernel(const __grid_con
     __syncwarp();
   } else {
     // ---------------- epilogue: TMEM -> registers -> HBM ----------------
+    // A block on qubit 0 keeps row pairs (2p, 2p+1) adjacent in HBM: each
+    // thread then writes them as one 16-byte store.
     const int q = warp & 3;  // TMEM lane quarter this warp may access
     const int h = (warp - EPI_WARP0) >> 2;  // block rows 32h .. 32h+31
     const int col = 32 * q + lane;
+    const bool pairs = a.bq[0] == 0;
     const int n_neg = n_neg_sh, n_other = n_other_sh;
     uint32_t i = 0;
     for (uint64_t t = first; t < ntiles; t += stride, ++i) {
@@ -460,21 +435,31 @@ __global__ void __launch_bounds__(blk::THREADS, 1) block_kernel(const __grid_con
         tmem_ld32(tl + 32 * h, re);
         tmem_ld32(tl + 64 + 32 * h, im);
         tc_wait_ld();
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(bar_dempty + 8 * b);  // accumulator read: the MMA may reuse it
         const uint32_t negh = (uint32_t)(neg >> (32 * h));
         float2* pc = a.amps + gc;
 #pragma unroll
-        for (int jj = 0; jj < 32; ++jj) {
-          float2 y = make_float2(re[jj], im[jj]);
-          if ((negh >> jj) & 1) y = make_float2(-y.x, -y.y);
-          const uint64_t gr = h ? a.grow[32 + jj] : a.grow[jj];
+        for (int jj = 0; jj < 32; jj += 2) {
+          float2 y0 = make_float2(re[jj], im[jj]), y1 = make_float2(re[jj + 1], im[jj + 1]);
+          if ((negh >> jj) & 1) y0 = make_float2(-y0.x, -y0.y);
+          if ((negh >> (jj + 1)) & 1) y1 = make_float2(-y1.x, -y1.y);
+          const uint64_t g0 = h ? a.grow[32 + jj] : a.grow[jj];
+          const uint64_t g1 = h ? a.grow[33 + jj] : a.grow[jj + 1];
           if (n_other)
-            for (int o = 0; o < n_other; ++o) y = apply_diag_op<float>(other_ops[o], y, gc | gr, a.coef, a.poly);
-          __stcs(pc + gr, y);
+            for (int o = 0; o < n_other; ++o) {
+              y0 = apply_diag_op<float>(other_ops[o], y0, gc | g0, a.coef, a.poly);
+              y1 = apply_diag_op<float>(other_ops[o], y1, gc | g1, a.coef, a.poly);
+            }
+          if (pairs) {
+            __stcs((float4*)(pc + g0), make_float4(y0.x, y0.y, y1.x, y1.y));
+          } else {
+            __stcs(pc + g0, y0);
+            __stcs(pc + g1, y1);
+          }
         }
       }
-      tc_fence_before();
-      __syncwarp();
-      if (lane == 0) mbar_arrive(bar_dempty + 8 * b);
     }
   }
 
@@ -483,6 +468,139 @@ __global__ void __launch_bounds__(blk::THREADS, 1) block_kernel(const __grid_con
   if (abort_sh && tid == 0) atomicExch(a.err, ALEPH_B200_DEVICE_FAILURE);
   if (warp == 0) tmem_dealloc(tmem, TMEM_COLS);
 }
+
+namespace {
+
+// Bank-conflict degree of one warp's 8-byte shared-memory accesses at byte
+// offsets off[0..32): the most distinct 4-byte words any of the 32 banks
+// serves (2 is the minimum: 256 bytes take two 128-byte wavefronts).
+int conflict_degree(const uint32_t* off) {
+  int worst = 0;
+  for (uint32_t bank = 0; bank < 32; ++bank) {
+    uint32_t words[64];
+    int nw = 0;
+    for (int t = 0; t < 32; ++t)
+      for (uint32_t h = 0; h < 2; ++h) {
+        const uint32_t w = off[t] / 4 + h;
+        if (w % 32 != bank) continue;
+        bool seen = false;
+        for (int k = 0; k < nw; ++k) seen = seen || words[k] == w;
+        if (!seen) words[nw++] = w;
+      }
+    worst = nw > worst ? nw : worst;
+  }
+  return worst;
+}
+
+// Tile geometry of a block pass. The tile qubits are the 6 block qubits plus
+// 7 column qubits; a tile is 2^(13-c) contiguous runs of 2^c amplitudes
+// (qubits 0..c-1 all in the tile), kept in a stage back to back, each run
+// followed by `pad` bytes. Column candidates: the 7 lowest non-block qubits,
+// and, for a block with a qubit below 7 that ends at or below qubit 12, the
+// non-block qubits under the block plus the ones above a one-qubit gap after
+// it (so that those columns index runs, which the pad skews across banks).
+// The candidate and pad with the fewest bank conflicts for the 32 columns of
+// a warp win (ties: the first, natural and unpadded).
+void set_tile_geometry(uint32_t n, const uint32_t* bq, BlockArgs* a) {
+  using namespace blk;
+  uint64_t bmask = 0;
+  uint32_t bmax = 0;
+  for (int j = 0; j < 6; ++j) {
+    bmask |= 1ull << bq[j];
+    bmax = bq[j] > bmax ? bq[j] : bmax;
+  }
+  uint32_t cand[2][7];
+  int ncand = 0;
+  {
+    int k = 0;
+    for (uint32_t q = 0; q < n && k < 7; ++q)
+      if (!((bmask >> q) & 1)) cand[ncand][k++] = q;
+    ++ncand;
+  }
+  if ((bmask & 0x7F) && bmax <= 12) {
+    int k = 0;
+    for (uint32_t q = 0; q < bmax; ++q)
+      if (!((bmask >> q) & 1)) cand[ncand][k++] = q;
+    for (uint32_t q = bmax + 2; q < n && k < 7; ++q) cand[ncand][k++] = q;
+    if (k == 7) ++ncand;
+  }
+  int best_deg = 1 << 30, best_c = 0;
+  uint32_t best_pad = 0;
+  for (int ci = 0; ci < ncand; ++ci) {
+    uint64_t tmask = bmask;
+    for (int k = 0; k < 7; ++k) tmask |= 1ull << cand[ci][k];
+    uint32_t c = 0;
+    while (c < 13 && ((tmask >> c) & 1)) ++c;
+    const uint32_t nruns = 1u << (13 - c), run_bytes = 8u << c;
+    for (uint32_t pad : {0u, 16u, 32u, 64u, 128u, 256u, 512u}) {
+      if (nruns * pad > (uint32_t)MAX_PAD_BYTES) break;
+      uint32_t off[32];
+      for (int t = 0; t < 32; ++t) {
+        off[t] = 0;
+        for (int k = 0; k < 5; ++k) {
+          if (!((t >> k) & 1)) continue;
+          const uint32_t pos = (uint32_t)__builtin_popcountll(tmask & ((1ull << cand[ci][k]) - 1));
+          off[t] += pos < c ? 8u << pos : (run_bytes + pad) << (pos - c);
+        }
+      }
+      const int deg = conflict_degree(off);
+      if (deg < best_deg) {
+        best_deg = deg;
+        best_c = ci;
+        best_pad = pad;
+      }
+    }
+  }
+  const uint32_t* cols = cand[best_c];
+  uint64_t tmask = bmask;
+  for (int k = 0; k < 7; ++k) tmask |= 1ull << cols[k];
+  uint32_t c = 0;
+  while (c < 13 && ((tmask >> c) & 1)) ++c;
+  a->tmask = tmask;
+  a->nruns = 1u << (13 - c);
+  a->run_bytes = 8u << c;
+  a->run_stride = a->run_bytes + best_pad;
+  auto stride = [&](uint32_t q) -> uint32_t {  // stage byte stride of tile qubit q
+    const uint32_t pos = (uint32_t)__builtin_popcountll(tmask & ((1ull << q) - 1));
+    return pos < c ? 8u << pos : a->run_stride << (pos - c);
+  };
+  for (uint32_t j = 0; j < 64; ++j) {
+    uint32_t ro = 0;
+    uint64_t gr = 0;
+    for (int b = 0; b < 6; ++b)
+      if ((j >> b) & 1) {
+        ro += stride(bq[b]);
+        gr |= 1ull << bq[b];
+      }
+    a->rowoff[j] = ro;
+    a->grow[j] = gr;
+  }
+  for (uint32_t col = 0; col < (uint32_t)NCOL; ++col) {
+    uint32_t co = 0;
+    uint64_t gc = 0;
+    for (int k = 0; k < 7; ++k)
+      if ((col >> k) & 1) {
+        co += stride(cols[k]);
+        gc |= 1ull << cols[k];
+      }
+    a->coloff[col] = co;
+    a->gcol[col] = gc;
+  }
+  for (uint32_t r = 0; r < (uint32_t)MAX_RUNS; ++r) {  // run r: its bits -> the tile qubits from c up
+    uint64_t off = 0;
+    if (r < a->nruns) {
+      uint32_t bit = 0;
+      for (uint32_t q = c; q < n; ++q)
+        if ((tmask >> q) & 1) {
+          if ((r >> bit) & 1) off |= 1ull << q;
+          ++bit;
+        }
+    }
+    a->runoff[r] = off;
+  }
+}
+
+}  // namespace
 
 cudaError_t launch_block_pass(void* amps, const BlockPass& p, const uint8_t* images, const Op* ops, const void* coef,
                               PolyTables poly, int* dev_error, int sm_count, cudaStream_t s) {
@@ -497,28 +615,7 @@ cudaError_t launch_block_pass(void* amps, const BlockPass& p, const uint8_t* ima
   a.err = dev_error;
   a.n = p.n;
   for (int j = 0; j < 6; ++j) a.bq[j] = p.bq[j];
-  {
-    // tile geometry, as in the kernel: T = block qubits + the 7 lowest other qubits
-    uint64_t bmask = 0;
-    for (int j = 0; j < 6; ++j) bmask |= 1ull << p.bq[j];
-    uint64_t tmask = bmask;
-    for (uint32_t q = 0, k = 0; q < p.n && k < 7; ++q)
-      if (!((bmask >> q) & 1)) {
-        tmask |= 1ull << q;
-        ++k;
-      }
-    for (uint32_t j = 0; j < 64; ++j) {
-      uint32_t lr = 0;
-      uint64_t gr = 0;
-      for (int b = 0; b < 6; ++b)
-        if ((j >> b) & 1) {
-          lr |= 1u << __builtin_popcountll(tmask & ((1ull << p.bq[b]) - 1));
-          gr |= 1ull << p.bq[b];
-        }
-      a.lrow[j] = lr;
-      a.grow[j] = gr;
-    }
-  }
+  set_tile_geometry(p.n, p.bq, &a);
   static bool attr = false;
   if (!attr) {
     cudaError_t e = cudaFuncSetAttribute(block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, blk::SMEM_BYTES);
