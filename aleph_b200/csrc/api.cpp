@@ -262,7 +262,8 @@ int execute(aleph_b200_handle* h, aleph_b200_state* st, const Plan& P, const dou
     if (e != cudaSuccess) return cuda_fail(h, e, "event record");
     switch (ps.kind) {
       case PASS_TILE:
-        e = launch_tile_pass(st->amps, st->precision, ps.tile, d.ops, d.coef, d.poly, h->stream);
+        e = launch_tile_pass(st->amps, st->precision, ps.tile, d.ops, d.coef, d.poly, (int*)(d.status + 4),
+                             h->sm_count, h->stream);
         h->stats.tile_passes++;
         h->stats.passes++;
         h->stats.algorithmic_bytes += 2 * len * bpa;
@@ -333,8 +334,8 @@ int execute(aleph_b200_handle* h, aleph_b200_state* st, const Plan& P, const dou
     if (P.n_measures)
       CK(copy_async(h, oc.data(), d.outcomes, P.n_measures, cudaMemcpyDeviceToHost, h->stream), "outcome readback");
     CK(cudaStreamSynchronize(h->stream), "stream synchronize");
-    if (stv[4] != 0)  // a tensor-core block pass gave up on a bounded wait
-      return set_error(h, ALEPH_B200_DEVICE_FAILURE, "device operation failed: block pass wait expired");
+    if (stv[4] != 0)  // a tile or block pass gave up on a bounded wait
+      return set_error(h, ALEPH_B200_DEVICE_FAILURE, "device operation failed: pass copy wait expired");
     if (status_out) *status_out = stv;
     if (outcomes_out) {
       oc.resize(P.n_measures);

@@ -169,8 +169,9 @@ inline __host__ __device__ double norm_tolerance(uint64_t len, int precision) {
 
 // kernels_*.cu entry points (host wrappers; all launch on `stream`)
 cudaError_t launch_init_zero_state(void* amps, uint32_t n, int precision, cudaStream_t s);
+// dev_error: set to ALEPH_B200_DEVICE_FAILURE by a pass kernel whose bounded copy wait expires.
 cudaError_t launch_tile_pass(void* amps, int precision, const TilePass& p, const Op* ops, const void* coef,
-                             PolyTables poly, cudaStream_t s);
+                             PolyTables poly, int* dev_error, int sm_count, cudaStream_t s);
 cudaError_t launch_smem_pass(void* amps, int precision, uint32_t n, const Op* ops, uint32_t op_count,
                              const void* coef, PolyTables poly, cudaStream_t s);
 cudaError_t launch_kq_pass(void* amps, int precision, uint32_t n, const Op* op_dev, const Op& op_host,

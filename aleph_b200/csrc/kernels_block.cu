@@ -616,11 +616,14 @@ cudaError_t launch_block_pass(void* amps, const BlockPass& p, const uint8_t* ima
   a.n = p.n;
   for (int j = 0; j < 6; ++j) a.bq[j] = p.bq[j];
   set_tile_geometry(p.n, p.bq, &a);
-  static bool attr = false;
-  if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, blk::SMEM_BYTES);
+  static uint64_t attr_devices = 0;  // devices on which the shared-memory opt-in is done
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev >= 64 || !((attr_devices >> dev) & 1)) {
+    e = cudaFuncSetAttribute(block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, blk::SMEM_BYTES);
     if (e != cudaSuccess) return e;
-    attr = true;
+    if (dev < 64) attr_devices |= 1ull << dev;
   }
   const uint64_t ntiles = 1ull << (p.n - 13);
   const unsigned grid = (unsigned)(ntiles < (uint64_t)sm_count ? ntiles : (uint64_t)sm_count);

@@ -317,7 +317,8 @@ static cudaError_t launch_tile_t(void* amps, const TilePass& p, const Op* ops, c
 }
 
 cudaError_t launch_tile_pass(void* amps, int precision, const TilePass& p, const Op* ops, const void* coef,
-                             PolyTables poly, cudaStream_t s) {
+                             PolyTables poly, int* /*dev_error: no waits in this kernel*/, int /*sm_count*/,
+                             cudaStream_t s) {
   if (p.R < 1 || p.R > 5 || p.n < 5 + p.R) return cudaErrorInvalidValue;
   const bool f64 = precision == ALEPH_B200_F64;
   switch (p.R) {
