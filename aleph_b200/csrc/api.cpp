@@ -1047,6 +1047,12 @@ int aleph_b200_set_tuning(aleph_b200_handle* h, const char* key, int64_t value) 
     h->record_passes = value != 0;
     return ALEPH_B200_OK;
   }
+  if (!std::strcmp(key, "tile_occupancy")) {
+    if (value != 0 && (value < 2 || value > 4))
+      return set_error(h, ALEPH_B200_INVALID_ARGUMENT, "tile_occupancy must be 0 or in 2..4");
+    h->opts.tile_occupancy = (uint32_t)value;
+    return ALEPH_B200_OK;
+  }
   if (!std::strcmp(key, "block_window_search")) {
     h->opts.block_window_search = value != 0;
     return ALEPH_B200_OK;

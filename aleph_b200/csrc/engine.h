@@ -60,7 +60,7 @@ struct TilePass {
   uint32_t hq[5];
   uint32_t op_begin;
   uint32_t op_count;
-  uint32_t pad;
+  uint32_t occupancy;  // resident 128-thread blocks per SM the kernel variant targets (2..4; 0 = default)
 };
 
 // Tensor-core dense-block pass (TC32): a 2^6 x 2^6 complex matrix on the
@@ -120,6 +120,7 @@ struct PlanOptions {
   bool tensor_blocks = false;   // TC32: fuse into 6-qubit dense blocks
   uint32_t block_k = 6;
   bool block_window_search = true;  // TC32: also try every 6-qubit window per pass
+  uint32_t tile_occupancy = 0;      // tile kernel variant: 128-thread blocks per SM (0 = 2)
 };
 
 // ---------------------------------------------------------------------------

@@ -251,10 +251,13 @@ __device__ __forceinline__ void dispatch_2q(const Op& op, V2<Real> (&v)[1 << R],
 }
 
 // ---- the warp-tile pass -----------------------------------------------------
-template <typename Real, int R>
-__global__ void __launch_bounds__(128) tile_kernel(V2<Real>* __restrict__ amps, const TilePass p,
-                                                   const Op* __restrict__ ops, const V2<Real>* __restrict__ coef,
-                                                   const PolyTables poly) {
+// OCC: the resident 128-thread blocks per SM the variant is compiled for
+// (register budget 65536 / (128 * OCC)); more resident warps hide more
+// latency, fewer registers per thread cost spills at large R.
+template <typename Real, int R, int OCC>
+__global__ void __launch_bounds__(128, OCC) tile_kernel(V2<Real>* __restrict__ amps, const TilePass p,
+                                                        const Op* __restrict__ ops, const V2<Real>* __restrict__ coef,
+                                                        const PolyTables poly) {
   constexpr int NR = 1 << R;
   const int lane = threadIdx.x & 31;
   const uint64_t warp = (uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
@@ -306,14 +309,29 @@ __global__ void __launch_bounds__(128) tile_kernel(V2<Real>* __restrict__ amps, 
   for (int r = 0; r < NR; ++r) st_amp<Real>(amps + (gl | roff<R>(r, hb)), v[r]);
 }
 
-template <typename Real, int R>
+template <typename Real, int R, int OCC>
 static cudaError_t launch_tile_t(void* amps, const TilePass& p, const Op* ops, const void* coef, PolyTables poly,
                                  cudaStream_t s) {
   const uint64_t warps = 1ull << (p.n - 5 - R);
   const uint32_t wpb = 4;
   const uint64_t blocks = (warps + wpb - 1) / wpb;
-  tile_kernel<Real, R><<<(unsigned)blocks, 32 * wpb, 0, s>>>((V2<Real>*)amps, p, ops, (const V2<Real>*)coef, poly);
+  tile_kernel<Real, R, OCC>
+      <<<(unsigned)blocks, 32 * wpb, 0, s>>>((V2<Real>*)amps, p, ops, (const V2<Real>*)coef, poly);
   return cudaGetLastError();
+}
+
+template <typename Real, int R>
+static cudaError_t launch_tile_occ(void* amps, const TilePass& p, const Op* ops, const void* coef, PolyTables poly,
+                                   cudaStream_t s) {
+  // default: FP32 tiles run best at 4 blocks per SM, FP64 at 2 (measured on
+  // the n=30 depth-40 brickwall: FP32 R=5 occ 2/3/4 = 1.22/1.00/0.94 s, FP64
+  // R=5 occ 2/3 = 1.57/1.63 s)
+  const uint32_t occ = p.occupancy ? p.occupancy : (sizeof(Real) == 4 ? 4u : 2u);
+  switch (occ) {
+    case 3: return launch_tile_t<Real, R, 3>(amps, p, ops, coef, poly, s);
+    case 4: return launch_tile_t<Real, R, 4>(amps, p, ops, coef, poly, s);
+    default: return launch_tile_t<Real, R, 2>(amps, p, ops, coef, poly, s);
+  }
 }
 
 cudaError_t launch_tile_pass(void* amps, int precision, const TilePass& p, const Op* ops, const void* coef,
@@ -322,12 +340,18 @@ cudaError_t launch_tile_pass(void* amps, int precision, const TilePass& p, const
   if (p.R < 1 || p.R > 5 || p.n < 5 + p.R) return cudaErrorInvalidValue;
   const bool f64 = precision == ALEPH_B200_F64;
   switch (p.R) {
-    case 1: return f64 ? launch_tile_t<double, 1>(amps, p, ops, coef, poly, s) : launch_tile_t<float, 1>(amps, p, ops, coef, poly, s);
-    case 2: return f64 ? launch_tile_t<double, 2>(amps, p, ops, coef, poly, s) : launch_tile_t<float, 2>(amps, p, ops, coef, poly, s);
-    case 3: return f64 ? launch_tile_t<double, 3>(amps, p, ops, coef, poly, s) : launch_tile_t<float, 3>(amps, p, ops, coef, poly, s);
-    case 4: return f64 ? launch_tile_t<double, 4>(amps, p, ops, coef, poly, s) : launch_tile_t<float, 4>(amps, p, ops, coef, poly, s);
-    default: return f64 ? launch_tile_t<double, 5>(amps, p, ops, coef, poly, s) : launch_tile_t<float, 5>(amps, p, ops, coef, poly, s);
+#define AB_TILE_CASE(RR)                                                        \
+  case RR:                                                                      \
+    return f64 ? launch_tile_occ<double, RR>(amps, p, ops, coef, poly, s)       \
+               : launch_tile_occ<float, RR>(amps, p, ops, coef, poly, s);
+    AB_TILE_CASE(1)
+    AB_TILE_CASE(2)
+    AB_TILE_CASE(3)
+    AB_TILE_CASE(4)
+    AB_TILE_CASE(5)
+#undef AB_TILE_CASE
   }
+  return cudaErrorInvalidValue;
 }
 
 }  // namespace ab

@@ -832,6 +832,8 @@ int build_plan(const std::vector<Lowered>& ops, uint32_t n, const PlanOptions& o
     }
   }
   flush();
+  for (Pass& ps : P->passes)
+    if (ps.kind == PASS_TILE) ps.tile.occupancy = o.tile_occupancy;
   return status;
 }
 
