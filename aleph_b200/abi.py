@@ -143,6 +143,10 @@ class PassRecord(ct.Structure):
     ]
 
 
+class QaoaSet(ct.Structure):
+    _fields_ = [("num_qubits", ct.c_uint32), ("num_edges", ct.c_uint32), ("edge_offset", ct.c_uint64)]
+
+
 class PlanConfig(ct.Structure):
     _fields_ = [
         ("precision", ct.c_int32),
@@ -188,6 +192,9 @@ _SIGNATURES = {
     "aleph_b200_norm_sqr": ([_P, _P, ct.POINTER(ct.c_double)], ct.c_int),
     "aleph_b200_synchronize": ([_P], ct.c_int),
     "aleph_b200_get_stream": ([_P, ct.POINTER(_P)], ct.c_int),
+    "aleph_b200_qaoa_sweep": (
+        [_P, ct.c_uint32, ct.POINTER(QaoaSet), ct.c_uint32, ct.POINTER(ct.c_uint32), ct.c_uint64,
+         ct.POINTER(ct.c_double), ct.POINTER(ct.c_double)], ct.c_int),
     "aleph_b200_describe_plan": (
         [ct.c_uint32, ct.POINTER(PlanConfig), ct.POINTER(Instr), ct.c_uint64, ct.POINTER(Pools),
          ct.POINTER(PassRecord), ct.c_uint64, ct.POINTER(ct.c_uint64)], ct.c_int),

@@ -252,6 +252,30 @@ class B200SvBackend:
         return [int(outs[i]) for i in range(nout.value)]
 
 
+    def qaoa_sweep(self, graphs, gammas, betas) -> np.ndarray:
+        """<C> of the build_qaoa Max-Cut circuit (crates/aleph-ir/src/ansatz.rs:71-117)
+        for every parameter set k: ``graphs[k] = (num_qubits, [(i, j), ...])``,
+        ``gammas[k]`` / ``betas[k]`` of one common length p. One persistent launch."""
+        count = len(graphs)
+        gam = np.asarray(gammas, dtype=np.float64).reshape(count, -1)
+        bet = np.asarray(betas, dtype=np.float64).reshape(count, -1)
+        if gam.shape != bet.shape:
+            raise ValueError("gammas and betas must have the same shape")
+        p = gam.shape[1]
+        sets = (abi.QaoaSet * max(1, count))()
+        pool = []
+        for k, (nq, edges) in enumerate(graphs):
+            sets[k].num_qubits, sets[k].num_edges, sets[k].edge_offset = nq, len(edges), len(pool) // 2
+            for (i, j) in edges:
+                pool += [int(i), int(j)]
+        edges_arr = np.ascontiguousarray(np.asarray(pool, dtype=np.uint32))
+        ang = np.ascontiguousarray(np.concatenate([gam, bet], axis=1))
+        out = np.zeros(max(1, count), dtype=np.float64)
+        self._check(self.lib.aleph_b200_qaoa_sweep(
+            self.handle, p, sets, count, edges_arr.ctypes.data_as(ct.POINTER(ct.c_uint32)) if edges_arr.size else None,
+            edges_arr.size // 2, ang.ctypes.data_as(ct.POINTER(ct.c_double)), out.ctypes.data_as(ct.POINTER(ct.c_double))))
+        return out[:count]
+
     def compile(self, num_qubits: int, instructions) -> "CompiledPlan":
         """``CudaExecutionPlan::compile`` (crates/aleph-cuda/src/execution.rs:78): validate
         and plan once; the plan tables stay resident on the device."""

@@ -6,6 +6,7 @@
 // is no host compute path: every amplitude update and every reduction runs
 // in the CUDA kernels of this library.
 
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -383,8 +384,11 @@ int aleph_b200_destroy(aleph_b200_handle* h) {
   if (!h) return ALEPH_B200_OK;
   cudaSetDevice(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
-  for (Scratch* s : {&h->reduce, &h->plan_buf, &h->sample, &h->status})
+  for (Scratch* s : {&h->reduce, &h->plan_buf, &h->sample, &h->status, &h->qaoa.dev, &h->qaoa.state, &h->qaoa.cuts})
     if (s->ptr) cudaFree(s->ptr);
+  if (h->qaoa.exec) cudaGraphExecDestroy(h->qaoa.exec);
+  if (h->qaoa.host_in) cudaFreeHost(h->qaoa.host_in);
+  if (h->qaoa.host_out) cudaFreeHost(h->qaoa.host_out);
   for (cudaEvent_t ev : h->events) cudaEventDestroy(ev);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete static_cast<FullHandle*>(h);
@@ -467,9 +471,9 @@ int aleph_b200_apply_gate(aleph_b200_handle* h, aleph_b200_state* st, const alep
   if (int r = bind(h)) return r;
   std::vector<Lowered> ops(1);
   aleph_b200_error_info e{};
-  if (int s = lower_gate(*g, st->n, pool, pool_len, &ops[0], &e)) return report(h, e);
+  if (lower_gate(*g, st->n, pool, pool_len, &ops[0], &e)) return report(h, e);
   Plan P;
-  build_plan(ops, st->n, h->opts, &P);
+  if (int s = build_plan(ops, st->n, h->opts, &P)) return set_error(h, s, "optimization pipeline failed: planner");
   return execute(h, st, P, nullptr, 0, nullptr, nullptr);
 }
 
@@ -558,7 +562,7 @@ static int run_plan(aleph_b200_handle* h, aleph_b200_state* st, const Plan& P, c
     e.status = stv[0];
     e.qubit = (uint32_t)stv[2];
     if (e.status == ALEPH_B200_INVALID_STATE)
-      std::snprintf(e.kind, sizeof(e.kind), "state norm deviates from 1 beyond drift budget");
+      std::snprintf(e.kind, sizeof(e.kind), "norm drifted beyond budget");
     else if (e.status == ALEPH_B200_INVALID_ARGUMENT)
       std::snprintf(e.kind, sizeof(e.kind), "measure uniforms exhausted");
     return report(h, e);
@@ -643,6 +647,141 @@ int aleph_b200_plan_free(aleph_b200_handle* h, aleph_b200_plan* plan) {
   return ALEPH_B200_OK;
 }
 
+int aleph_b200_qaoa_sweep(aleph_b200_handle* h, uint32_t p, const aleph_b200_qaoa_set* sets, uint32_t n_sets,
+                          const uint32_t* edges, uint64_t n_edge_pairs, const double* angles, double* expectations) {
+  if (!h || (n_sets && (!sets || !angles || !expectations)) || (n_edge_pairs && !edges)) return ALEPH_B200_INVALID_ARGUMENT;
+  if (p == 0) return set_error(h, ALEPH_B200_INVALID_ARGUMENT, "qaoa sweep needs p >= 1 layers");
+  if (n_sets == 0) return ALEPH_B200_OK;
+  // validation, in the reference's order for one circuit: qubit count, then
+  // each edge's CNOT(i, j) operands, then the Rz / Rx angles
+  const int prec = h->precision == ALEPH_B200_F64 ? ALEPH_B200_F64 : ALEPH_B200_F32;
+  const uint32_t smem_n = qaoa_smem_max_n(prec);
+  uint32_t nmax_stream = 0;
+  for (uint32_t k = 0; k < n_sets; ++k) {
+    const aleph_b200_qaoa_set& s = sets[k];
+    aleph_b200_error_info e{};
+    e.instruction = k;
+    if (s.num_qubits == 0 || s.num_qubits > 26) {
+      e.status = ALEPH_B200_TOO_MANY_QUBITS;
+      e.requested = s.num_qubits;
+      e.limit = 26;
+      if (s.num_qubits == 0) return set_error(h, ALEPH_B200_INVALID_ARGUMENT, "qaoa set %u has no qubits", k);
+      return report(h, e);
+    }
+    if (s.num_edges > 128 || s.edge_offset + s.num_edges > n_edge_pairs)
+      return set_error(h, ALEPH_B200_INVALID_ARGUMENT, "qaoa set %u: edge range outside the edge pool (or > 128)", k);
+    for (uint32_t j = 0; j < s.num_edges; ++j) {
+      const uint32_t u = edges[2 * (s.edge_offset + j)], v = edges[2 * (s.edge_offset + j) + 1];
+      if (u >= s.num_qubits || v >= s.num_qubits) {
+        e.status = ALEPH_B200_QUBIT_OUT_OF_RANGE;
+        e.qubit = u >= s.num_qubits ? u : v;
+        e.num_qubits = s.num_qubits;
+        return report(h, e);
+      }
+      if (u == v) {
+        e.status = ALEPH_B200_DUPLICATE_QUBIT;
+        e.qubit = u;
+        return report(h, e);
+      }
+    }
+    for (uint32_t j = 0; j < 2 * p; ++j)
+      if (!std::isfinite(angles[(size_t)2 * p * k + j])) {
+        e.status = ALEPH_B200_NON_FINITE_PARAM;
+        std::snprintf(e.kind, sizeof(e.kind), j < p ? "rz" : "rx");
+        return report(h, e);
+      }
+    if (s.num_qubits > smem_n && s.num_qubits > nmax_stream) nmax_stream = s.num_qubits;
+  }
+  if (int r = bind(h)) return r;
+  auto& Q = h->qaoa;
+  // streamed sets: one state slice and one cut slice per CTA, within a memory budget
+  const uint64_t slice = nmax_stream ? (1ull << nmax_stream) : 0;
+  const size_t bpa = prec == ALEPH_B200_F64 ? 16 : 8;
+  int grid = h->sm_count;
+  if (slice) {
+    const uint64_t budget = 48ull << 30;
+    const uint64_t per_cta = slice * (bpa + 1);
+    if ((uint64_t)grid * per_cta > budget) grid = (int)(budget / per_cta);
+    if (grid < 1) grid = 1;
+  }
+  // device input region: sets | order | edges | angles | out | counter
+  const size_t b_sets = al((size_t)n_sets * sizeof(aleph_b200_qaoa_set)), b_order = al((size_t)n_sets * 4),
+               b_edges = al((size_t)n_edge_pairs * 8), b_ang = al((size_t)n_sets * 2 * p * 8),
+               b_out = al((size_t)n_sets * 8), b_cnt = al(4);
+  const size_t in_bytes = b_sets + b_order + b_edges + b_ang;
+  const size_t total = in_bytes + b_out + b_cnt;
+  const uint64_t key[6] = {(uint64_t)prec, n_sets, p, n_edge_pairs, (uint64_t)grid, slice};
+  const bool same = Q.exec && std::memcmp(key, Q.key, sizeof(key)) == 0;
+  if (!same) {
+    if (Q.exec) {
+      cudaGraphExecDestroy(Q.exec);
+      Q.exec = nullptr;
+    }
+    if (int r = ensure(h, Q.dev, total)) return r;
+    if (slice) {
+      if (int r = ensure(h, Q.state, (size_t)grid * slice * bpa)) return r;
+      if (int r = ensure(h, Q.cuts, (size_t)grid * slice)) return r;
+    }
+    if (Q.host_in_bytes < in_bytes) {
+      if (Q.host_in) cudaFreeHost(Q.host_in);
+      Q.host_in = nullptr;
+      Q.host_in_bytes = 0;
+      CK(cudaHostAlloc(&Q.host_in, in_bytes, cudaHostAllocDefault), "pinned staging");
+      Q.host_in_bytes = in_bytes;
+    }
+    if (Q.host_out_bytes < b_out) {
+      if (Q.host_out) cudaFreeHost(Q.host_out);
+      Q.host_out = nullptr;
+      Q.host_out_bytes = 0;
+      CK(cudaHostAlloc(&Q.host_out, b_out, cudaHostAllocDefault), "pinned staging");
+      Q.host_out_bytes = b_out;
+    }
+  }
+  // stage this call's inputs (the graph copies the staging area as it is at replay)
+  uint8_t* hin = (uint8_t*)Q.host_in;
+  std::memcpy(hin, sets, (size_t)n_sets * sizeof(aleph_b200_qaoa_set));
+  {
+    std::vector<uint32_t> order(n_sets);
+    for (uint32_t k = 0; k < n_sets; ++k) order[k] = k;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](uint32_t x, uint32_t y) { return sets[x].num_qubits > sets[y].num_qubits; });
+    std::memcpy(hin + b_sets, order.data(), (size_t)n_sets * 4);
+  }
+  if (n_edge_pairs) std::memcpy(hin + b_sets + b_order, edges, (size_t)n_edge_pairs * 8);
+  std::memcpy(hin + b_sets + b_order + b_edges, angles, (size_t)n_sets * 2 * p * 8);
+  char* d = (char*)Q.dev.ptr;
+  if (!same) {
+    // capture: inputs up, counter cleared, the persistent sweep, results down
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal), "graph capture");
+    cudaError_t e = cudaMemcpyAsync(d, hin, in_bytes, cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d + in_bytes + b_out, 0, 4, h->stream);
+    if (e == cudaSuccess)
+      e = launch_qaoa_sweep(prec, (const aleph_b200_qaoa_set*)d, (const uint32_t*)(d + b_sets + b_order),
+                            (const double*)(d + b_sets + b_order + b_edges), (const uint32_t*)(d + b_sets),
+                            (uint32_t*)(d + in_bytes + b_out), (double*)(d + in_bytes), Q.state.ptr,
+                            (uint8_t*)Q.cuts.ptr, slice, n_sets, p, grid, h->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(Q.host_out, d + in_bytes, (size_t)n_sets * 8, cudaMemcpyDeviceToHost, h->stream);
+    const cudaError_t ec = cudaStreamEndCapture(h->stream, &g);
+    if (e == cudaSuccess) e = ec;
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&Q.exec, g, 0);
+    if (g) cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+      Q.exec = nullptr;
+      cudaGetLastError();
+      return cuda_fail(h, e, "qaoa sweep graph");
+    }
+    std::memcpy(Q.key, key, sizeof(key));
+  }
+  CK(cudaGraphLaunch(Q.exec, h->stream), "qaoa sweep graph launch");
+  CK(cudaStreamSynchronize(h->stream), "stream synchronize");
+  std::memcpy(expectations, Q.host_out, (size_t)n_sets * 8);
+  h->stats.kernel_launches += 1;
+  h->stats.h2d_bytes += in_bytes;
+  h->stats.d2h_bytes += (size_t)n_sets * 8;
+  return ALEPH_B200_OK;
+}
+
 int aleph_b200_apply_diagonal_phase(aleph_b200_handle* h, aleph_b200_state* st, const aleph_b200_phase_term* terms,
                                     uint64_t n_terms, const uint64_t* conds, uint64_t n_conds) {
   if (!h || !st || (!terms && n_terms)) return ALEPH_B200_INVALID_ARGUMENT;
@@ -720,7 +859,6 @@ static int check_norm_host(aleph_b200_handle* h, aleph_b200_state* st, double* n
   CK(copy_async(h, res, out2, 16, cudaMemcpyDeviceToHost, h->stream), "norm readback");
   CK(cudaStreamSynchronize(h->stream), "stream synchronize");
   if (norm_out) *norm_out = res[0];
-  const double len = (double)(1ull << st->n);
   if (res[1] > 0.0) {
     aleph_b200_error_info e{};
     e.status = ALEPH_B200_INVALID_STATE;

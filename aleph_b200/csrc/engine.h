@@ -158,6 +158,17 @@ struct Handle {
   bool record_passes = false;
   std::vector<cudaEvent_t> events;
   std::vector<aleph_b200_pass_record> records;
+  // batched QAOA sweep: device buffers, pinned staging and the captured graph
+  struct Qaoa {
+    Scratch dev;           // sets | order | edges | angles | out | counter
+    Scratch state;         // per-CTA state slices (streamed sets)
+    Scratch cuts;          // per-CTA cut(z) slices
+    void* host_in = nullptr;   // pinned staging of the device input region
+    void* host_out = nullptr;  // pinned staging of the results
+    size_t host_in_bytes = 0, host_out_bytes = 0;
+    cudaGraphExec_t exec = nullptr;
+    uint64_t key[6] = {0, 0, 0, 0, 0, 0};  // layout the graph was captured for
+  } qaoa;
 };
 
 // Accepted |sum |a|^2 - 1| of a state before readout: the FP64 drift budget
@@ -197,6 +208,14 @@ cudaError_t launch_expectation(const void* amps, int precision, uint32_t n, uint
 cudaError_t launch_probabilities(const void* amps, int precision, uint32_t n, const uint32_t* qubits_dev, uint32_t k,
                                  double* partials, uint32_t nblocks, double* out, double* norm_out, cudaStream_t s);
 uint32_t reduce_blocks(uint32_t n, int sm_count);
+
+// batched QAOA sweep (kernels_qaoa.cu): sets with n <= qaoa_smem_max_n run in
+// shared memory; larger ones stream through per-CTA slices of slice_amps.
+uint32_t qaoa_smem_max_n(int precision);
+cudaError_t launch_qaoa_sweep(int precision, const aleph_b200_qaoa_set* sets, const uint32_t* edges,
+                              const double* angles, const uint32_t* order, uint32_t* next, double* out,
+                              void* scratch, uint8_t* cuts, uint64_t slice_amps, uint32_t n_sets, uint32_t p,
+                              int grid, cudaStream_t s);
 
 // sampling (kernels_sample.cu)
 size_t sample_scratch_bytes(uint32_t n, int mode, uint32_t shots);

@@ -1,0 +1,263 @@
+// kernels_qaoa.cu — batched QAOA Max-Cut sweep: many parameter sets with
+// ragged qubit counts in one persistent launch.
+//
+// Circuit of one set (build_qaoa, crates/aleph-ir/src/ansatz.rs:71-98): H on
+// every qubit, then p layers of [CNOT(i,j) Rz(2 gamma)_j CNOT(i,j) per edge,
+// Rx(2 beta) on every qubit]. On a basis state z the edge gadget is the phase
+// exp(-i gamma (1 - 2 [z_i != z_j])), so a cost layer is the diagonal
+// exp(-i gamma (m - 2 cut(z))) with m edges; a mixer layer is Rx(2 beta) on
+// every qubit. The output is <C> = sum_z |psi_z|^2 cut(z), the expectation of
+// H_C = sum_edges 1/2 (I - Z_i Z_j) (ansatz.rs:100-117), reduced in FP64.
+//
+// One CTA per SM pulls sets from a queue (largest first). A state of at most
+// SMEM_N qubits lives in shared memory for the whole circuit. A larger one
+// lives in the CTA's slice of a device buffer and is streamed in tiles of
+// 2^13 amplitudes, two passes per layer: pass A over contiguous chunks
+// (qubits 0..12: cost phase + mixer), pass B over tiles spanning the qubits
+// 13..n-1 (mixer). The first pass generates |+>^n instead of reading it; the
+// last pass only reads and accumulates <C>.
+//
+// cut(z) per amplitude: within a pass-A chunk z = (t << 13) | lo and
+// cut(z) = cutT[lo] + (edges among the high qubits cut by t) + X0[lo & 127] +
+// X1[lo >> 7], where cutT counts the edges among qubits 0..12 (per set) and
+// X0 / X1 the edges between a low and a high qubit (per chunk). The first
+// cost layer also stores cut(z) as one byte per amplitude, which the final
+// pass B reads. Multiple edges between the same pair count once each, as the
+// repeated gadgets do.
+
+#include "common.cuh"
+
+namespace ab {
+
+namespace qaoa {
+
+constexpr int THREADS = 512;
+constexpr int TILE_BITS = 13;
+constexpr uint32_t TILE = 1u << TILE_BITS;
+constexpr int MAX_EDGES = 128;
+template <typename Real>
+struct Cfg {
+  static constexpr int SMEM_N = sizeof(Real) == 4 ? 14 : 13;  // states kept in shared memory
+  static constexpr uint32_t SMEM_BYTES = (1u << SMEM_N) * sizeof(V2<Real>);
+};
+
+struct Args {
+  const aleph_b200_qaoa_set* sets;
+  const uint32_t* edges;   // (u, v) pairs
+  const double* angles;    // per set: gamma[0..p), beta[0..p)
+  const uint32_t* order;   // set indices, largest first
+  uint32_t* next;          // work counter (zero at launch)
+  double* out;
+  void* scratch;           // per-CTA state slices for the streamed sets
+  uint8_t* cuts;           // per-CTA cut(z) slices
+  uint64_t slice_amps;
+  uint32_t n_sets, p;
+};
+
+// Rx(2 beta) on tile-local bit k of every pair in S[0..len): (a, b) -> (c a - i s b, c b - i s a).
+template <typename Real>
+__device__ __forceinline__ void mixer_bit(V2<Real>* S, uint32_t len, uint32_t k, Real c, Real s) {
+  for (uint32_t i = threadIdx.x; i < len / 2; i += THREADS) {
+    const uint32_t j0 = (uint32_t)insert_zero(i, k), j1 = j0 | (1u << k);
+    const V2<Real> a = S[j0], b = S[j1];
+    S[j0] = mk<Real>(c * a.x + s * b.y, c * a.y - s * b.x);
+    S[j1] = mk<Real>(c * b.x + s * a.y, c * b.y - s * a.x);
+  }
+}
+
+__device__ __forceinline__ double block_sum(double v, double* red) {
+  for (int o = 16; o; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double s = 0.0;
+  if (threadIdx.x == 0)
+    for (int w = 0; w < THREADS / 32; ++w) s += red[w];
+  __syncthreads();
+  return s;
+}
+
+template <typename Real>
+__global__ void __launch_bounds__(THREADS, 1) sweep_kernel(Args a) {
+  extern __shared__ __align__(16) uint8_t qsm[];
+  V2<Real>* S = (V2<Real>*)qsm;
+  __shared__ uint8_t eu[MAX_EDGES], ev[MAX_EDGES];
+  __shared__ uint8_t cutT[1 << 14];
+  __shared__ uint8_t X0[128], X1[64];
+  __shared__ V2<Real> ph[MAX_EDGES + 1];  // cost-layer phase by cut value
+  __shared__ double red[THREADS / 32];
+  __shared__ uint32_t s_idx, s_ch;
+  const uint32_t tid = threadIdx.x;
+  V2<Real>* X = (V2<Real>*)a.scratch + (uint64_t)blockIdx.x * a.slice_amps;
+  uint8_t* CG = a.cuts + (uint64_t)blockIdx.x * a.slice_amps;
+
+  for (;;) {
+    if (tid == 0) s_idx = atomicAdd(a.next, 1u);
+    __syncthreads();
+    const uint32_t idx = s_idx;
+    __syncthreads();
+    if (idx >= a.n_sets) break;
+    const uint32_t ci = a.order[idx];
+    const aleph_b200_qaoa_set cs = a.sets[ci];
+    const uint32_t n = cs.num_qubits, m = cs.num_edges;
+    for (uint32_t e = tid; e < m; e += THREADS) {
+      eu[e] = (uint8_t)a.edges[2 * (cs.edge_offset + e)];
+      ev[e] = (uint8_t)a.edges[2 * (cs.edge_offset + e) + 1];
+    }
+    __syncthreads();
+    const bool in_smem = n <= (uint32_t)Cfg<Real>::SMEM_N;
+    const uint32_t lb = in_smem ? n : (uint32_t)TILE_BITS;  // cutT covers qubits 0..lb-1
+    for (uint32_t z = tid; z < (1u << lb); z += THREADS) {
+      uint32_t c = 0;
+      for (uint32_t e = 0; e < m; ++e)
+        if (eu[e] < lb && ev[e] < lb) c += ((z >> eu[e]) ^ (z >> ev[e])) & 1u;
+      cutT[z] = (uint8_t)c;
+    }
+    const double* gam = a.angles + (size_t)ci * 2 * a.p;
+    const double* bet = gam + a.p;
+    const uint64_t len = 1ull << n;
+    const Real amp0 = (Real)rsqrt((double)len);  // |+>^n
+    auto set_phases = [&](double gamma) {  // ph[k] = exp(-i gamma (m - 2k))
+      __syncthreads();
+      for (uint32_t k = tid; k <= m; k += THREADS) {
+        double sn, cn;
+        sincos(-gamma * ((double)m - 2.0 * (double)k), &sn, &cn);
+        ph[k] = mk<Real>((Real)cn, (Real)sn);
+      }
+      __syncthreads();
+    };
+    double acc = 0.0;
+
+    if (in_smem) {
+      // ---- whole state in shared memory ----
+      const uint32_t L = (uint32_t)len;
+      for (uint32_t i = tid; i < L; i += THREADS) S[i] = mk<Real>(amp0, (Real)0);
+      for (uint32_t l = 0; l < a.p; ++l) {
+        set_phases(gam[l]);
+        for (uint32_t i = tid; i < L; i += THREADS) S[i] = cmul<Real>(ph[cutT[i]], S[i]);
+        double sb, cb;
+        sincos(bet[l], &sb, &cb);
+        for (uint32_t k = 0; k < n; ++k) {
+          __syncthreads();
+          mixer_bit<Real>(S, L, k, (Real)cb, (Real)sb);
+        }
+        __syncthreads();
+      }
+      for (uint32_t i = tid; i < L; i += THREADS) {
+        const double x = (double)S[i].x, y = (double)S[i].y;
+        acc += (x * x + y * y) * (double)cutT[i];
+      }
+    } else {
+      // ---- streamed through this CTA's state slice ----
+      const uint32_t h = n - TILE_BITS;     // qubits 13..n-1
+      const uint32_t c = TILE_BITS - h;     // pass B: low run bits (n <= 26)
+      const uint64_t ntiles = len >> TILE_BITS;
+      for (uint32_t l = 0; l < a.p; ++l) {
+        set_phases(gam[l]);
+        double sb, cb;
+        sincos(bet[l], &sb, &cb);
+        const Real rc = (Real)cb, rs = (Real)sb;
+        // pass A: contiguous chunks, cost phase + mixer on qubits 0..12
+        for (uint64_t t = 0; t < ntiles; ++t) {
+          // chunk constants: cut edges among the high qubits, and the low/high cross-edge tables
+          if (tid == 0) {
+            uint32_t ch = 0;
+            for (uint32_t e = 0; e < m; ++e)
+              if (eu[e] >= TILE_BITS && ev[e] >= TILE_BITS)
+                ch += (uint32_t)(((t >> (eu[e] - TILE_BITS)) ^ (t >> (ev[e] - TILE_BITS))) & 1u);
+            s_ch = ch;
+          }
+          if (tid < 192) {
+            const uint32_t base = tid < 128 ? 0u : 7u, v = tid < 128 ? tid : tid - 128;
+            uint32_t x = 0;
+            for (uint32_t e = 0; e < m; ++e) {
+              const uint32_t u0 = eu[e], v0 = ev[e];
+              const bool ul = u0 < TILE_BITS, vl = v0 < TILE_BITS;
+              if (ul == vl) continue;  // not a low/high cross edge
+              const uint32_t lo_q = ul ? u0 : v0, hi_q = ul ? v0 : u0;
+              if (lo_q < base || lo_q >= base + (base ? 6u : 7u)) continue;
+              const uint32_t zb = (v >> (lo_q - base)) & 1u, hb = (uint32_t)(t >> (hi_q - TILE_BITS)) & 1u;
+              x += zb ^ hb;
+            }
+            if (tid < 128) X0[v] = (uint8_t)x;
+            else X1[v] = (uint8_t)x;
+          }
+          __syncthreads();
+          const uint32_t ch = s_ch;
+          const uint64_t g0 = t << TILE_BITS;
+          for (uint32_t i = tid; i < TILE; i += THREADS) {
+            const uint32_t cut = cutT[i] + ch + X0[i & 127] + X1[i >> 7];
+            if (l == 0) CG[g0 + i] = (uint8_t)cut;
+            const V2<Real> v = l == 0 ? mk<Real>(amp0, (Real)0) : X[g0 + i];
+            S[i] = cmul<Real>(ph[cut], v);
+          }
+          for (uint32_t k = 0; k < (uint32_t)TILE_BITS; ++k) {
+            __syncthreads();
+            mixer_bit<Real>(S, TILE, k, rc, rs);
+          }
+          __syncthreads();
+          for (uint32_t i = tid; i < TILE; i += THREADS) X[g0 + i] = S[i];
+          __syncthreads();
+        }
+        // pass B: tiles over {qubits 0..c-1} + {qubits 13..n-1}; tile index -> qubits c..12
+        const bool last = l + 1 == a.p;
+        for (uint64_t t = 0; t < ntiles; ++t) {
+          auto gidx = [&](uint32_t i) -> uint64_t {
+            const uint64_t lo = i & ((1u << c) - 1), hi = i >> c;
+            return lo | (t << c) | (hi << TILE_BITS);
+          };
+          for (uint32_t i = tid; i < TILE; i += THREADS) S[i] = X[gidx(i)];
+          for (uint32_t k = 0; k < h; ++k) {
+            __syncthreads();
+            mixer_bit<Real>(S, TILE, c + k, rc, rs);
+          }
+          __syncthreads();
+          if (last) {
+            for (uint32_t i = tid; i < TILE; i += THREADS) {
+              const double x = (double)S[i].x, y = (double)S[i].y;
+              acc += (x * x + y * y) * (double)CG[gidx(i)];
+            }
+          } else {
+            for (uint32_t i = tid; i < TILE; i += THREADS) X[gidx(i)] = S[i];
+          }
+          __syncthreads();
+        }
+      }
+    }
+    const double tot = block_sum(acc, red);
+    if (tid == 0) a.out[ci] = tot;
+    __syncthreads();
+  }
+}
+
+}  // namespace qaoa
+
+uint32_t qaoa_smem_max_n(int precision) {
+  return precision == ALEPH_B200_F64 ? (uint32_t)qaoa::Cfg<double>::SMEM_N : (uint32_t)qaoa::Cfg<float>::SMEM_N;
+}
+
+cudaError_t launch_qaoa_sweep(int precision, const aleph_b200_qaoa_set* sets, const uint32_t* edges,
+                              const double* angles, const uint32_t* order, uint32_t* next, double* out,
+                              void* scratch, uint8_t* cuts, uint64_t slice_amps, uint32_t n_sets, uint32_t p,
+                              int grid, cudaStream_t s) {
+  qaoa::Args a{sets, edges, angles, order, next, out, scratch, cuts, slice_amps, n_sets, p};
+  static uint64_t attr_devices[2] = {0, 0};  // per precision: devices with the shared-memory opt-in
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  const int k = precision == ALEPH_B200_F64 ? 1 : 0;
+  if (dev >= 64 || !((attr_devices[k] >> dev) & 1)) {
+    e = k ? cudaFuncSetAttribute(qaoa::sweep_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 qaoa::Cfg<double>::SMEM_BYTES)
+          : cudaFuncSetAttribute(qaoa::sweep_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 qaoa::Cfg<float>::SMEM_BYTES);
+    if (e != cudaSuccess) return e;
+    if (dev < 64) attr_devices[k] |= 1ull << dev;
+  }
+  if (k)
+    qaoa::sweep_kernel<double><<<grid, qaoa::THREADS, qaoa::Cfg<double>::SMEM_BYTES, s>>>(a);
+  else
+    qaoa::sweep_kernel<float><<<grid, qaoa::THREADS, qaoa::Cfg<float>::SMEM_BYTES, s>>>(a);
+  return cudaGetLastError();
+}
+
+}  // namespace ab

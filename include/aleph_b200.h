@@ -219,6 +219,27 @@ int aleph_b200_execute(aleph_b200_handle* h, aleph_b200_state* st, aleph_b200_pl
                        uint64_t* n_outcomes);
 int aleph_b200_plan_free(aleph_b200_handle* h, aleph_b200_plan* plan);
 
+/* ---- batched QAOA Max-Cut sweep ----
+ * Evaluates <C> = <psi|H_C|psi>, H_C = sum_edges 1/2 (I - Z_i Z_j)
+ * (maxcut_pauli_sum, crates/aleph-ir/src/ansatz.rs:100-117), for many
+ * parameter sets at once; set k's state is the build_qaoa circuit
+ * (ansatz.rs:71-98) on sets[k].num_qubits qubits with the edges
+ * edges[2e], edges[2e+1] for e in [edge_offset, edge_offset + num_edges) and
+ * the angles angles[2p k .. 2p k + p) (gammas) and angles[2p k + p .. 2p(k+1))
+ * (betas). The state precision is the handle's (F64: complex128; F32 and
+ * TC32: complex64); <C> is reduced in FP64 either way. All sets run in one
+ * persistent launch, replayed as a CUDA graph while the batch layout
+ * (counts, sizes) stays the same. Limits: 1 <= num_qubits <= 26, num_edges
+ * <= 128, p >= 1. Errors: QubitOutOfRange / DuplicateQubit for a bad edge
+ * (the reference's CNOT(i, j) checks), NonFiniteParam, TooManyQubits. */
+typedef struct aleph_b200_qaoa_set {
+  uint32_t num_qubits;
+  uint32_t num_edges;
+  uint64_t edge_offset; /* in (u, v) pairs */
+} aleph_b200_qaoa_set;
+int aleph_b200_qaoa_sweep(aleph_b200_handle* h, uint32_t p, const aleph_b200_qaoa_set* sets, uint32_t n_sets,
+                          const uint32_t* edges, uint64_t n_edge_pairs, const double* angles, double* expectations);
+
 /* ---- Backend::apply_diagonal_phase (crates/aleph-sv/src/kernels/diagonal_phase.rs:74-97) ---- */
 int aleph_b200_apply_diagonal_phase(aleph_b200_handle* h, aleph_b200_state* st, const aleph_b200_phase_term* terms,
                                     uint64_t n_terms, const uint64_t* cond_pool, uint64_t n_conds);
