@@ -137,6 +137,10 @@ class PassRecord(ct.Structure):
         ("nq", ct.c_uint32),
         ("qubits", ct.c_uint32 * 8),
         ("post_ops", ct.c_uint32),
+        ("lane_ops", ct.c_uint32),
+        ("dense_ops", ct.c_uint32),
+        ("diag_ops", ct.c_uint32),
+        ("variant", ct.c_uint32),
         ("pad", ct.c_uint32),
         ("ms", ct.c_double),
         ("bytes", ct.c_double),
@@ -153,6 +157,7 @@ class PlanConfig(ct.Structure):
         ("tile_r", ct.c_uint32),
         ("smem_max_n", ct.c_uint32),
         ("block_window_search", ct.c_uint32),
+        ("tile_occupancy", ct.c_uint32),
     ]
 
 
@@ -192,6 +197,15 @@ _SIGNATURES = {
     "aleph_b200_norm_sqr": ([_P, _P, ct.POINTER(ct.c_double)], ct.c_int),
     "aleph_b200_synchronize": ([_P], ct.c_int),
     "aleph_b200_get_stream": ([_P, ct.POINTER(_P)], ct.c_int),
+    "aleph_b200_mlp_create": ([_P, ct.c_uint32, ct.c_uint32, ct.c_uint64, ct.POINTER(_P)], ct.c_int),
+    "aleph_b200_mlp_free": ([_P, _P], ct.c_int),
+    "aleph_b200_mlp_params": ([_P, _P, ct.POINTER(ct.c_float), ct.POINTER(ct.c_float), ct.POINTER(ct.c_uint64)],
+                              ct.c_int),
+    "aleph_b200_mlp_predict": ([_P, _P, ct.POINTER(ct.c_float), ct.c_uint32, ct.POINTER(ct.c_float)], ct.c_int),
+    "aleph_b200_mlp_gradients": ([_P, _P, ct.POINTER(ct.c_float), ct.POINTER(ct.c_float), ct.c_uint32,
+                                  ct.POINTER(ct.c_float), ct.POINTER(ct.c_float)], ct.c_int),
+    "aleph_b200_mlp_train": ([_P, _P, ct.POINTER(ct.c_float), ct.POINTER(ct.c_float), ct.c_uint32, ct.c_uint32,
+                              ct.c_uint32, ct.c_float, ct.c_uint64, ct.POINTER(ct.c_float)], ct.c_int),
     "aleph_b200_qaoa_sweep": (
         [_P, ct.c_uint32, ct.POINTER(QaoaSet), ct.c_uint32, ct.POINTER(ct.c_uint32), ct.c_uint64,
          ct.POINTER(ct.c_double), ct.POINTER(ct.c_double)], ct.c_int),

@@ -233,11 +233,7 @@ class B200SvBackend:
         self.lib.aleph_b200_get_pass_records(self.handle, None, 0, ct.byref(n))
         buf = (abi.PassRecord * max(1, n.value))()
         self._check(self.lib.aleph_b200_get_pass_records(self.handle, buf, n.value, ct.byref(n)))
-        out = []
-        for r in buf[: n.value]:
-            out.append({"kind": abi.PASS_KINDS.get(r.kind, r.kind), "gates": r.gates, "n": r.n,
-                        "qubits": list(r.qubits[: r.nq]), "post_ops": r.post_ops, "ms": r.ms, "bytes": r.bytes})
-        return out
+        return [_record_dict(r) for r in buf[: n.value]]
 
     def apply_stream(self, state: State, instructions, measure_uniforms=None, flat: Flat | None = None):
         """Apply a whole instruction list in one call; returns measurement outcomes."""
@@ -250,7 +246,6 @@ class B200SvBackend:
             u.ctypes.data_as(ct.POINTER(ct.c_double)) if u is not None and u.size else None,
             0 if u is None else u.size, outs, flat.n, ct.byref(nout)))
         return [int(outs[i]) for i in range(nout.value)]
-
 
     def qaoa_sweep(self, graphs, gammas, betas) -> np.ndarray:
         """<C> of the build_qaoa Max-Cut circuit (crates/aleph-ir/src/ansatz.rs:71-117)
@@ -286,6 +281,12 @@ class B200SvBackend:
         return CompiledPlan(p, num_qubits, flat, self)
 
 
+def _record_dict(r) -> dict:
+    return {"kind": abi.PASS_KINDS.get(r.kind, r.kind), "gates": r.gates, "n": r.n, "qubits": list(r.qubits[: r.nq]),
+            "post_ops": r.post_ops, "lane_ops": r.lane_ops, "dense_ops": r.dense_ops, "diag_ops": r.diag_ops,
+            "variant": r.variant, "ms": r.ms, "bytes": r.bytes}
+
+
 class CompiledPlan:
     """A plan compiled by :meth:`B200SvBackend.compile`; ``execute`` applies it
     (``CudaExecutionPlan::execute``, crates/aleph-cuda/src/execution.rs:183)."""
@@ -317,11 +318,11 @@ class CompiledPlan:
 
 
 def describe_plan(num_qubits: int, instructions, precision: str = "f64", tile_r: int = 5, smem_max_n: int = 12,
-                  block_window_search: bool = True) -> list[dict]:
+                  block_window_search: bool = True, tile_occupancy: int = 0) -> list[dict]:
     """The passes the planner makes of ``instructions`` (host only, no device)."""
     lib = abi.load_library()
     flat = instructions if isinstance(instructions, Flat) else flatten(instructions)
-    cfg = abi.PlanConfig(abi.PRECISION[precision], tile_r, smem_max_n, int(bool(block_window_search)))
+    cfg = abi.PlanConfig(abi.PRECISION[precision], tile_r, smem_max_n, int(bool(block_window_search)), tile_occupancy)
     n = ct.c_uint64()
     st = lib.aleph_b200_describe_plan(num_qubits, ct.byref(cfg), flat.instrs, flat.n, ct.byref(flat.pools), None, 0,
                                       ct.byref(n))
@@ -330,8 +331,7 @@ def describe_plan(num_qubits: int, instructions, precision: str = "f64", tile_r:
     buf = (abi.PassRecord * max(1, n.value))()
     lib.aleph_b200_describe_plan(num_qubits, ct.byref(cfg), flat.instrs, flat.n, ct.byref(flat.pools), buf, n.value,
                                  ct.byref(n))
-    return [{"kind": abi.PASS_KINDS.get(r.kind, r.kind), "gates": r.gates, "n": r.n, "qubits": list(r.qubits[: r.nq]),
-             "post_ops": r.post_ops, "bytes": r.bytes} for r in buf[: n.value]]
+    return [_record_dict(r) for r in buf[: n.value]]
 
 
 def run_with_outcomes(backend: B200SvBackend, circuit: Circuit, measure_uniforms=None):

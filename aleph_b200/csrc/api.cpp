@@ -305,6 +305,13 @@ int execute(aleph_b200_handle* h, aleph_b200_state* st, const Plan& P, const dou
       const double bytes = ps.kind == PASS_MEASURE ? 3 * len * bpa : 2 * len * bpa;
       CK(record_end(pk, (uint32_t)ps.kind, ps.gates, nq, qs, ps.kind == PASS_BLOCK ? ps.block.post_count : 0, bytes),
          "event record");
+      if (rec) {
+        aleph_b200_pass_record& r = h->records.back();
+        r.lane_ops = ps.lane_ops;
+        r.dense_ops = ps.dense_ops;
+        r.diag_ops = ps.diag_ops;
+        r.variant = ps.kind == PASS_TILE ? ps.tile.occupancy : 0;
+      }
     }
     ++pk;
   }
@@ -1191,6 +1198,12 @@ int aleph_b200_set_tuning(aleph_b200_handle* h, const char* key, int64_t value) 
     h->opts.tile_occupancy = (uint32_t)value;
     return ALEPH_B200_OK;
   }
+  if (!std::strcmp(key, "tensor_blocks")) {
+    if (h->precision != ALEPH_B200_TC32)
+      return set_error(h, ALEPH_B200_INVALID_ARGUMENT, "tensor_blocks applies to TC32 handles only");
+    h->opts.tensor_blocks = value != 0;
+    return ALEPH_B200_OK;
+  }
   if (!std::strcmp(key, "block_window_search")) {
     h->opts.block_window_search = value != 0;
     return ALEPH_B200_OK;
@@ -1208,13 +1221,15 @@ int aleph_b200_describe_plan(uint32_t num_qubits, const aleph_b200_plan_config* 
                              uint64_t* n_passes) {
   if (!config || !n_passes || (!in && count) || (cap && !out)) return ALEPH_B200_INVALID_ARGUMENT;
   if (config->precision < ALEPH_B200_F64 || config->precision > ALEPH_B200_TC32 || config->tile_r < 1 ||
-      config->tile_r > 5 || config->smem_max_n > 12 || num_qubits > 40)
+      config->tile_r > 5 || config->smem_max_n > 12 || num_qubits > 40 ||
+      (config->tile_occupancy != 0 && (config->tile_occupancy < 2 || config->tile_occupancy > 4)))
     return ALEPH_B200_INVALID_ARGUMENT;
   FullHandle tmp;  // host-only: validation messages land here, no device is touched
   tmp.opts.tile_r = config->tile_r;
   tmp.opts.smem_max_n = config->smem_max_n;
   tmp.opts.tensor_blocks = config->precision == ALEPH_B200_TC32;
   tmp.opts.block_window_search = config->block_window_search != 0;
+  tmp.opts.tile_occupancy = config->tile_occupancy;
   std::vector<Lowered> ops;
   if (int r = lower_stream(&tmp, num_qubits, in, count, pools, &ops)) return r;
   Plan P;
@@ -1232,6 +1247,10 @@ int aleph_b200_describe_plan(uint32_t num_qubits, const aleph_b200_plan_config* 
     r.nq = ps.kind == PASS_BLOCK ? 6 : ps.kind == PASS_TILE ? ps.tile.R : 0;
     for (uint32_t j = 0; j < r.nq && j < 8; ++j) r.qubits[j] = qs[j];
     r.post_ops = ps.kind == PASS_BLOCK ? ps.block.post_count : 0;
+    r.lane_ops = ps.lane_ops;
+    r.dense_ops = ps.dense_ops;
+    r.diag_ops = ps.diag_ops;
+    r.variant = ps.kind == PASS_TILE ? ps.tile.occupancy : 0;
     r.bytes = (ps.kind == PASS_MEASURE ? 3 : 2) * len * bpa;
     out[k] = r;
   }
@@ -1254,6 +1273,198 @@ int aleph_b200_get_stats(const aleph_b200_handle* h, aleph_b200_stats* out) {
 int aleph_b200_reset_stats(aleph_b200_handle* h) {
   if (!h) return ALEPH_B200_INVALID_ARGUMENT;
   h->stats = aleph_b200_stats{};
+  return ALEPH_B200_OK;
+}
+
+// ---- the learned planner's cost model (kernels_mlp.cu) -------------------------
+struct aleph_b200_mlp {
+  int F = 0, H = 0;
+  size_t np = 0;
+  Scratch params, grads, adam_m, adam_v;  // np floats each
+  Scratch work;                           // X | y | activations | backward scratch | loss
+  int step = 0;
+};
+
+namespace {
+// Work region for a batch of B samples: X (B F) | y (B) | acts (3 B H + B) | dbuf (2 B H) | loss.
+size_t mlp_work_floats(int B, int F, int H) {
+  return (size_t)B * F + B + (size_t)3 * B * H + B + (size_t)2 * B * H + 4;
+}
+int mlp_upload_batch(aleph_b200_handle* h, aleph_b200_mlp* m, const float* X, const float* y, int B) {
+  if (int r = ensure(h, m->work, mlp_work_floats(B, m->F, m->H) * 4)) return r;
+  float* w = (float*)m->work.ptr;
+  CK(copy_async(h, w, X, (size_t)B * m->F * 4, cudaMemcpyHostToDevice, h->stream), "mlp batch upload");
+  if (y) CK(copy_async(h, w + (size_t)B * m->F, y, (size_t)B * 4, cudaMemcpyHostToDevice, h->stream), "mlp target upload");
+  return 0;
+}
+}  // namespace
+
+int aleph_b200_mlp_create(aleph_b200_handle* h, uint32_t n_features, uint32_t hidden, uint64_t seed,
+                          aleph_b200_mlp** out) {
+  if (!h || !out || n_features == 0 || n_features > 1024 || hidden == 0 || hidden > 1024)
+    return ALEPH_B200_INVALID_ARGUMENT;
+  *out = nullptr;
+  if (int r = bind(h)) return r;
+  aleph_b200_mlp* m = new (std::nothrow) aleph_b200_mlp();
+  if (!m) return set_error(h, ALEPH_B200_DEVICE_FAILURE, "host allocation failed");
+  m->F = (int)n_features;
+  m->H = (int)hidden;
+  m->np = mlp_param_count(m->F, m->H);
+  // He-uniform weights (bound sqrt(6 / fan_in)), zero biases, from a splitmix64 stream
+  std::vector<float> p(m->np, 0.f);
+  uint64_t x = seed;
+  const int ins[4] = {m->F, m->H, m->H, m->H}, outs[4] = {m->H, m->H, m->H, 1};
+  size_t off = 0;
+  for (int l = 0; l < 4; ++l) {
+    const float bound = std::sqrt(6.f / (float)ins[l]);
+    for (size_t k = 0; k < (size_t)ins[l] * outs[l]; ++k) {
+      const double u = (double)(splitmix64(x) >> 11) * (1.0 / 9007199254740992.0);
+      p[off + k] = (float)((2.0 * u - 1.0) * bound);
+    }
+    off += (size_t)ins[l] * outs[l] + outs[l];
+  }
+  int r = ensure(h, m->params, m->np * 4);
+  if (!r) r = ensure(h, m->grads, m->np * 4);
+  if (!r) r = ensure(h, m->adam_m, m->np * 4);
+  if (!r) r = ensure(h, m->adam_v, m->np * 4);
+  if (r) {
+    for (Scratch* s : {&m->params, &m->grads, &m->adam_m, &m->adam_v})
+      if (s->ptr) cudaFree(s->ptr);
+    delete m;
+    return r;
+  }
+  cudaError_t e = copy_async(h, m->params.ptr, p.data(), m->np * 4, cudaMemcpyHostToDevice, h->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(m->adam_m.ptr, 0, m->np * 4, h->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(m->adam_v.ptr, 0, m->np * 4, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) {
+    for (Scratch* s : {&m->params, &m->grads, &m->adam_m, &m->adam_v})
+      if (s->ptr) cudaFree(s->ptr);
+    delete m;
+    return cuda_fail(h, e, "mlp init");
+  }
+  *out = m;
+  return ALEPH_B200_OK;
+}
+
+int aleph_b200_mlp_free(aleph_b200_handle* h, aleph_b200_mlp* m) {
+  if (!m) return ALEPH_B200_OK;
+  if (h) {
+    cudaSetDevice(h->device);
+    cudaStreamSynchronize(h->stream);
+  }
+  for (Scratch* s : {&m->params, &m->grads, &m->adam_m, &m->adam_v, &m->work})
+    if (s->ptr) cudaFree(s->ptr);
+  delete m;
+  return ALEPH_B200_OK;
+}
+
+int aleph_b200_mlp_params(aleph_b200_handle* h, aleph_b200_mlp* m, float* get, const float* set, uint64_t* count) {
+  if (!h || !m) return ALEPH_B200_INVALID_ARGUMENT;
+  if (count) *count = m->np;
+  if (int r = bind(h)) return r;
+  if (set) {
+    CK(copy_async(h, m->params.ptr, set, m->np * 4, cudaMemcpyHostToDevice, h->stream), "mlp params upload");
+    CK(cudaMemsetAsync(m->adam_m.ptr, 0, m->np * 4, h->stream), "adam reset");
+    CK(cudaMemsetAsync(m->adam_v.ptr, 0, m->np * 4, h->stream), "adam reset");
+    m->step = 0;
+  }
+  if (get) CK(copy_async(h, get, m->params.ptr, m->np * 4, cudaMemcpyDeviceToHost, h->stream), "mlp params readback");
+  CK(cudaStreamSynchronize(h->stream), "stream synchronize");
+  return ALEPH_B200_OK;
+}
+
+int aleph_b200_mlp_predict(aleph_b200_handle* h, aleph_b200_mlp* m, const float* X, uint32_t n, float* y_out) {
+  if (!h || !m || (n && (!X || !y_out))) return ALEPH_B200_INVALID_ARGUMENT;
+  if (int r = bind(h)) return r;
+  const int F = m->F, H = m->H;
+  for (uint32_t b0 = 0; b0 < n; b0 += 4096) {
+    const int B = (int)std::min<uint32_t>(4096, n - b0);
+    if (int r = mlp_upload_batch(h, m, X + (size_t)b0 * F, nullptr, B)) return r;
+    float* w = (float*)m->work.ptr;
+    float* acts = w + (size_t)B * F + B;
+    CK(mlp_forward((const float*)m->params.ptr, w, acts, B, F, H, h->stream), "mlp forward");
+    CK(copy_async(h, y_out + b0, acts + (size_t)3 * B * H, (size_t)B * 4, cudaMemcpyDeviceToHost, h->stream),
+       "mlp readback");
+    CK(cudaStreamSynchronize(h->stream), "stream synchronize");
+  }
+  h->stats.kernel_launches += 4;
+  return ALEPH_B200_OK;
+}
+
+int aleph_b200_mlp_gradients(aleph_b200_handle* h, aleph_b200_mlp* m, const float* X, const float* y, uint32_t n,
+                             float* grads_out, float* loss_out) {
+  if (!h || !m || !X || !y || !n || n > 65536) return ALEPH_B200_INVALID_ARGUMENT;
+  if (int r = bind(h)) return r;
+  const int F = m->F, H = m->H, B = (int)n;
+  if (int r = mlp_upload_batch(h, m, X, y, B)) return r;
+  float* w = (float*)m->work.ptr;
+  float* acts = w + (size_t)B * F + B;
+  float* dbuf = acts + (size_t)3 * B * H + B;
+  float* loss = dbuf + (size_t)2 * B * H;
+  CK(mlp_forward((const float*)m->params.ptr, w, acts, B, F, H, h->stream), "mlp forward");
+  CK(mlp_backward((const float*)m->params.ptr, w, acts, w + (size_t)B * F, (float*)m->grads.ptr, dbuf, loss, B, F, H,
+                  h->stream),
+     "mlp backward");
+  if (grads_out) CK(copy_async(h, grads_out, m->grads.ptr, m->np * 4, cudaMemcpyDeviceToHost, h->stream), "grad readback");
+  if (loss_out) CK(copy_async(h, loss_out, loss, 4, cudaMemcpyDeviceToHost, h->stream), "loss readback");
+  CK(cudaStreamSynchronize(h->stream), "stream synchronize");
+  return ALEPH_B200_OK;
+}
+
+int aleph_b200_mlp_train(aleph_b200_handle* h, aleph_b200_mlp* m, const float* X, const float* y, uint32_t n,
+                         uint32_t epochs, uint32_t batch, float lr, uint64_t seed, float* final_loss) {
+  if (!h || !m || !X || !y || !n || !batch || batch > 65536 || !(lr > 0.f)) return ALEPH_B200_INVALID_ARGUMENT;
+  if (int r = bind(h)) return r;
+  const int F = m->F, H = m->H;
+  const int B = (int)std::min<uint32_t>(batch, n);
+  // the whole data set lives on the device, reshuffled on the host once per epoch
+  Scratch data;
+  if (int r = ensure(h, data, (size_t)n * (F + 1) * 4)) return r;
+  if (int r = ensure(h, m->work, mlp_work_floats(B, F, H) * 4)) {
+    cudaFree(data.ptr);
+    return r;
+  }
+  std::vector<uint32_t> perm(n);
+  for (uint32_t i = 0; i < n; ++i) perm[i] = i;
+  std::vector<float> hx((size_t)n * F), hy(n);
+  uint64_t rs = seed;
+  float* dX = (float*)data.ptr;
+  float* dY = dX + (size_t)n * F;
+  float* w = (float*)m->work.ptr;
+  float* acts = w + (size_t)B * F + B;
+  float* dbuf = acts + (size_t)3 * B * H + B;
+  float* loss = dbuf + (size_t)2 * B * H;
+  float last = 0.f;
+  cudaError_t e = cudaSuccess;
+  for (uint32_t ep = 0; ep < epochs && e == cudaSuccess; ++ep) {
+    for (uint32_t i = n - 1; i > 0; --i) std::swap(perm[i], perm[splitmix64(rs) % (i + 1)]);  // Fisher-Yates
+    for (uint32_t i = 0; i < n; ++i) {
+      std::memcpy(&hx[(size_t)i * F], X + (size_t)perm[i] * F, (size_t)F * 4);
+      hy[i] = y[perm[i]];
+    }
+    e = copy_async(h, dX, hx.data(), hx.size() * 4, cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess) e = copy_async(h, dY, hy.data(), hy.size() * 4, cudaMemcpyHostToDevice, h->stream);
+    for (uint32_t b0 = 0; b0 + (uint32_t)B <= n && e == cudaSuccess; b0 += B) {
+      const float* xb = dX + (size_t)b0 * F;
+      const float* yb = dY + b0;
+      e = mlp_forward((const float*)m->params.ptr, xb, acts, B, F, H, h->stream);
+      if (e == cudaSuccess)
+        e = mlp_backward((const float*)m->params.ptr, xb, acts, yb, (float*)m->grads.ptr, dbuf, loss, B, F, H,
+                         h->stream);
+      if (e == cudaSuccess)
+        e = mlp_adam((float*)m->params.ptr, (const float*)m->grads.ptr, (float*)m->adam_m.ptr, (float*)m->adam_v.ptr,
+                     m->np, lr, ++m->step, h->stream);
+      h->stats.kernel_launches += 16;
+    }
+    // every epoch's host data is staged before the next shuffle overwrites it
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  }
+  if (e == cudaSuccess) e = copy_async(h, &last, loss, 4, cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  cudaFree(data.ptr);
+  if (e != cudaSuccess) return cuda_fail(h, e, "mlp training");
+  if (final_loss) *final_loss = last;
   return ALEPH_B200_OK;
 }
 

@@ -82,6 +82,8 @@ struct Pass {
   uint32_t qubit;      // PASS_MEASURE
   uint32_t record;     // instruction index (errors, outcome slot)
   uint32_t gates;      // gates consumed (stats / cost model)
+  // cost-model features: non-diagonal ops on lane qubits, all non-diagonal ops, diagonal ops
+  uint32_t lane_ops = 0, dense_ops = 0, diag_ops = 0;
 };
 
 // ---------------------------------------------------------------------------
@@ -208,6 +210,14 @@ cudaError_t launch_expectation(const void* amps, int precision, uint32_t n, uint
 cudaError_t launch_probabilities(const void* amps, int precision, uint32_t n, const uint32_t* qubits_dev, uint32_t k,
                                  double* partials, uint32_t nblocks, double* out, double* norm_out, cudaStream_t s);
 uint32_t reduce_blocks(uint32_t n, int sm_count);
+
+// learned planner cost model (kernels_mlp.cu): F -> H -> H -> H -> 1 MLP
+size_t mlp_param_count(int F, int H);
+cudaError_t mlp_forward(const float* params, const float* X, float* acts, int B, int F, int H, cudaStream_t s);
+cudaError_t mlp_backward(const float* params, const float* X, const float* acts, const float* y, float* grads,
+                         float* dbuf, float* loss_dev, int B, int F, int H, cudaStream_t s);
+cudaError_t mlp_adam(float* params, const float* grads, float* m, float* v, size_t n, float lr, int step,
+                     cudaStream_t s);
 
 // batched QAOA sweep (kernels_qaoa.cu): sets with n <= qaoa_smem_max_n run in
 // shared memory; larger ones stream through per-CTA slices of slice_amps.

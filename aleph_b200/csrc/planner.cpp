@@ -460,6 +460,18 @@ uint32_t append_op(Plan* P, const Lowered& L, Op op) {
   return (uint32_t)(P->ops.size() - 1);
 }
 
+// Cost-model features of a pass from the ops it applies.
+void count_ops(const std::vector<const Lowered*>& ops, Pass* ps) {
+  for (const Lowered* L : ops) {
+    if (L->nondiag) {
+      ++ps->dense_ops;
+      if (L->nondiag & 0x1Full) ++ps->lane_ops;
+    } else {
+      ++ps->diag_ops;
+    }
+  }
+}
+
 // Swap the operand order of a 4x4 matrix (MSB <-> LSB).
 void swap_2q_operands(std::vector<double>& c) {
   std::vector<double> out(c.size());
@@ -485,6 +497,7 @@ int plan_segment_tiles(const std::vector<const Lowered*>& seg, uint32_t n, uint3
       ps.tile.op_count = 1;
       ps.record = head->record;
       ps.gates = 1;
+      ps.dense_ops = 1;
       P->passes.push_back(ps);
       pending.erase(pending.begin());
       continue;
@@ -587,6 +600,7 @@ int plan_segment_tiles(const std::vector<const Lowered*>& seg, uint32_t n, uint3
     ps.tile = tp;
     ps.record = take.empty() ? 0 : take.front()->record;
     ps.gates = (uint32_t)take.size();
+    count_ops(take, &ps);
     P->passes.push_back(ps);
     pending.swap(rest);
   }
@@ -787,6 +801,9 @@ int plan_segment_blocks(const std::vector<const Lowered*>& seg, uint32_t n, uint
     ps.block.post_count = (uint32_t)P->ops.size() - ps.block.post_begin;
     ps.record = take.front()->record;
     ps.gates = (uint32_t)(take.size() + post.size());
+    count_ops(take, &ps);
+    ps.lane_ops = 0;  // a block has no lane shuffles
+    ps.diag_ops += (uint32_t)post.size();
     P->passes.push_back(ps);
     pending.swap(rest);
   }
@@ -809,6 +826,7 @@ int build_plan(const std::vector<Lowered>& ops, uint32_t n, const PlanOptions& o
       ps.tile.op_count = (uint32_t)P->ops.size() - ps.tile.op_begin;
       ps.record = seg.front()->record;
       ps.gates = (uint32_t)seg.size();
+      count_ops(seg, &ps);
       P->passes.push_back(ps);
     } else {
       // a 2-qubit gate may need two register qubits: R >= 2 unless only one high qubit exists

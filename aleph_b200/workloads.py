@@ -94,6 +94,65 @@ def qaoa_maxcut(n: int, edges, gammas, betas) -> C.Circuit:
     return c
 
 
+def _toffoli_ct(c: C.Circuit, a: int, b: int, t: int) -> None:
+    """Toffoli(a, b -> t) in CX, T, Tdg and H (the standard 6-CX circuit)."""
+    c.add(C.H(), [t])
+    c.add(C.Cnot(), [b, t]).add(C.Tdg(), [t]).add(C.Cnot(), [a, t]).add(C.T(), [t])
+    c.add(C.Cnot(), [b, t]).add(C.Tdg(), [t]).add(C.Cnot(), [a, t])
+    c.add(C.T(), [b]).add(C.T(), [t]).add(C.H(), [t])
+    c.add(C.Cnot(), [a, b]).add(C.T(), [a]).add(C.Tdg(), [b]).add(C.Cnot(), [a, b])
+
+
+def _mcz_ct(c: C.Circuit, qs: list[int], anc: list[int]) -> None:
+    """Z controlled on all of qs (|1..1> gets -1) with a V-chain of Toffolis
+    through the ancillas (computed, used, uncomputed), each in CX + T gates."""
+    if len(qs) == 1:
+        c.add(C.Z(), [qs[0]])
+        return
+    if len(qs) == 2:
+        c.add(C.Cz(), qs)
+        return
+    *ctrl, t = qs
+    c.add(C.H(), [t])
+    if len(ctrl) == 2:
+        _toffoli_ct(c, ctrl[0], ctrl[1], t)
+    else:
+        chain = [(ctrl[0], ctrl[1], anc[0])]
+        for i in range(2, len(ctrl) - 1):
+            chain.append((ctrl[i], anc[i - 2], anc[i - 1]))
+        for g in chain:
+            _toffoli_ct(c, *g)
+        _toffoli_ct(c, ctrl[-1], anc[len(ctrl) - 3], t)
+        for g in reversed(chain):
+            _toffoli_ct(c, *g)
+    c.add(C.H(), [t])
+
+
+def grover(n_data: int, marked: int, iterations: int) -> C.Circuit:
+    """Grover search over n_data qubits for the bitstring `marked`, with the
+    oracle's and the diffuser's multi-controlled Z decomposed into CX and T
+    gates through n_data - 2 ancillas (qubits n_data .. 2 n_data - 3)."""
+    n = max(n_data, 2 * n_data - 2)
+    c = C.Circuit(n)
+    data = list(range(n_data))
+    anc = list(range(n_data, n))
+    for q in data:
+        c.add(C.H(), [q])
+    for _ in range(iterations):
+        zeros = [q for q in data if not (marked >> q) & 1]
+        for q in zeros:
+            c.add(C.X(), [q])
+        _mcz_ct(c, data, anc)
+        for q in zeros:
+            c.add(C.X(), [q])
+        for q in data:
+            c.add(C.H(), [q]).add(C.X(), [q])
+        _mcz_ct(c, data, anc)
+        for q in data:
+            c.add(C.X(), [q]).add(C.H(), [q])
+    return c
+
+
 def maxcut_terms(edges):
     """<C> = sum_edges 1/2 (1 - <Z_i Z_j>) (crates/aleph-ir/src/ansatz.rs:105-117)."""
     return [((i, "Z"), (j, "Z")) for (i, j) in edges]

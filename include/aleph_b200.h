@@ -317,6 +317,10 @@ typedef struct aleph_b200_pass_record {
   uint32_t nq;          /* entries used in qubits[]                                        */
   uint32_t qubits[8];   /* tile register qubits / block qubits                             */
   uint32_t post_ops;    /* diagonal ops after a block                                      */
+  uint32_t lane_ops;    /* tile pass: non-diagonal ops on the lane qubits 0..4 (shuffles)  */
+  uint32_t dense_ops;   /* non-diagonal ops the pass applies (a block: the fused gates)    */
+  uint32_t diag_ops;    /* diagonal ops the pass applies (phases, CZ-like, DiagonalPhase)  */
+  uint32_t variant;     /* kernel variant (tile pass: blocks per SM)                       */
   uint32_t pad;
   double ms;            /* device time of the pass (CUDA events on the handle's stream)    */
   double bytes;         /* algorithmic HBM bytes of the pass                               */
@@ -331,6 +335,7 @@ typedef struct aleph_b200_plan_config {
   uint32_t tile_r;               /* register qubits per warp tile (1..5)     */
   uint32_t smem_max_n;           /* n <= this: one shared-memory pass        */
   uint32_t block_window_search;  /* TC32: also try every 6-qubit window      */
+  uint32_t tile_occupancy;       /* tile kernel variant: 0 (default) or 2..4 */
 } aleph_b200_plan_config;
 int aleph_b200_describe_plan(uint32_t num_qubits, const aleph_b200_plan_config* config, const aleph_b200_instr* instrs,
                              uint64_t count, const aleph_b200_pools* pools, aleph_b200_pass_record* out, uint64_t cap,
@@ -338,6 +343,26 @@ int aleph_b200_describe_plan(uint32_t num_qubits, const aleph_b200_plan_config* 
 /* Records of the last gate stream run with "record_passes" on; *n = count. */
 int aleph_b200_get_pass_records(const aleph_b200_handle* h, aleph_b200_pass_record* out, uint64_t cap,
                                 uint64_t* n);
+
+/* ---- the learned fusion planner's cost model: an FP32 MLP ----
+ * n_features -> hidden -> hidden -> hidden -> 1 (ReLU hidden layers), trained
+ * with MSE loss and Adam by this library's CUDA kernels on pass features and
+ * recorded pass times. No counterpart in the reference (its fusion is a
+ * greedy heuristic, crates/aleph-ir/src/passes/fuse_kq.rs:268-400).
+ * X is row-major n x n_features; y has n entries. */
+typedef struct aleph_b200_mlp aleph_b200_mlp;
+int aleph_b200_mlp_create(aleph_b200_handle* h, uint32_t n_features, uint32_t hidden, uint64_t seed,
+                          aleph_b200_mlp** out);
+int aleph_b200_mlp_free(aleph_b200_handle* h, aleph_b200_mlp* m);
+/* Parameter count into *count; copies them out (get) and/or replaces them (set). */
+int aleph_b200_mlp_params(aleph_b200_handle* h, aleph_b200_mlp* m, float* get, const float* set, uint64_t* count);
+int aleph_b200_mlp_predict(aleph_b200_handle* h, aleph_b200_mlp* m, const float* X, uint32_t n, float* y_out);
+/* Loss and parameter gradients of one batch (n <= 65536), without an update. */
+int aleph_b200_mlp_gradients(aleph_b200_handle* h, aleph_b200_mlp* m, const float* X, const float* y, uint32_t n,
+                             float* grads_out, float* loss_out);
+/* Mini-batch Adam for `epochs` passes over the (seed-shuffled) data; the last batch's loss in *final_loss. */
+int aleph_b200_mlp_train(aleph_b200_handle* h, aleph_b200_mlp* m, const float* X, const float* y, uint32_t n,
+                         uint32_t epochs, uint32_t batch, float lr, uint64_t seed, float* final_loss);
 
 /* ---- launch statistics (execution_counters, crates/aleph-cuda/src/execution.rs:145-165) ---- */
 typedef struct aleph_b200_stats {

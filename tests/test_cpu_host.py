@@ -194,3 +194,32 @@ def test_describe_plan_reports_validation_errors():
     with pytest.raises(BackendError) as e:
         describe_plan(4, [C.GateInstance(C.H(), [4])])
     assert e.value.status == abi.QUBIT_OUT_OF_RANGE
+
+
+# ---- learned planner: host logic ---------------------------------------------------------
+def test_learned_candidates_and_features():
+    from aleph_b200 import learned
+    from aleph_b200.backend import describe_plan
+
+    for prec in ("f64", "f32", "tc32"):
+        cs = learned.candidates(prec)
+        assert len(set(cs)) == len(cs) and cs[0] == learned.GREEDY
+    assert any(not c.tensor_blocks for c in learned.candidates("tc32"))
+    c = workloads.brickwall(24, 12, seed=3)
+    recs = describe_plan(24, c.instructions, "tc32")
+    X = np.stack([learned.pass_features(r, "tc32") for r in recs])
+    assert X.shape == (len(recs), learned.N_FEATURES) and np.isfinite(X).all()
+    assert (X[:, 1] == 1).all()  # every pass is a tensor-core block
+    assert sum(r["dense_ops"] + r["diag_ops"] for r in recs) == c.gate_count()
+    t = describe_plan(24, c.instructions, "f64", tile_r=4, tile_occupancy=3)
+    assert all(r["variant"] == 3 and len(r["qubits"]) == 4 for r in t)
+    assert sum(r["dense_ops"] + r["diag_ops"] for r in t) == c.gate_count()
+
+
+def test_grover_workload_amplifies_the_marked_state():
+    for nd, marked, it in [(3, 5, 1), (5, 17, 3)]:
+        c = workloads.grover(nd, marked, it)
+        psi, _ = oracle.run(c.num_qubits, c.instructions)
+        p = (np.abs(psi) ** 2).reshape(-1, 1 << nd)
+        assert p[0, marked] > 0.75  # ancillas back in |0>, marked state amplified
+        assert abs(p[1:].sum()) < 1e-12
