@@ -704,7 +704,7 @@ int aleph_b200_qaoa_sweep(aleph_b200_handle* h, uint32_t p, const aleph_b200_qao
   // streamed sets: one state slice and one cut slice per CTA, within a memory budget
   const uint64_t slice = nmax_stream ? (1ull << nmax_stream) : 0;
   const size_t bpa = prec == ALEPH_B200_F64 ? 16 : 8;
-  int grid = h->sm_count;
+  int grid = h->sm_count * qaoa_ctas_per_sm(prec);
   if (slice) {
     const uint64_t budget = 48ull << 30;
     const uint64_t per_cta = slice * (bpa + 1);

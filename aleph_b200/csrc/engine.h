@@ -222,6 +222,7 @@ cudaError_t mlp_adam(float* params, const float* grads, float* m, float* v, size
 // batched QAOA sweep (kernels_qaoa.cu): sets with n <= qaoa_smem_max_n run in
 // shared memory; larger ones stream through per-CTA slices of slice_amps.
 uint32_t qaoa_smem_max_n(int precision);
+int qaoa_ctas_per_sm(int precision);
 cudaError_t launch_qaoa_sweep(int precision, const aleph_b200_qaoa_set* sets, const uint32_t* edges,
                               const double* angles, const uint32_t* order, uint32_t* next, double* out,
                               void* scratch, uint8_t* cuts, uint64_t slice_amps, uint32_t n_sets, uint32_t p,

@@ -31,14 +31,17 @@ namespace ab {
 
 namespace qaoa {
 
-constexpr int THREADS = 512;
+constexpr int THREADS = 256;
 constexpr int TILE_BITS = 13;
 constexpr uint32_t TILE = 1u << TILE_BITS;
 constexpr int MAX_EDGES = 128;
 template <typename Real>
 struct Cfg {
-  static constexpr int SMEM_N = sizeof(Real) == 4 ? 14 : 13;  // states kept in shared memory
+  static constexpr int SMEM_N = 13;  // states kept in shared memory (the tile size)
   static constexpr uint32_t SMEM_BYTES = (1u << SMEM_N) * sizeof(V2<Real>);
+  // FP32 tiles (64 KiB) leave room for two CTAs per SM, which overlap one
+  // CTA's tile loads with the other's arithmetic
+  static constexpr int CTAS_PER_SM = sizeof(Real) == 4 ? 2 : 1;
 };
 
 struct Args {
@@ -65,6 +68,45 @@ __device__ __forceinline__ void mixer_bit(V2<Real>* S, uint32_t len, uint32_t k,
   }
 }
 
+// Rx(2 beta) on tile-local bits k0 < k1 of every quartet: one shared-memory
+// sweep for two qubits (the four amplitudes of a quartet in registers).
+template <typename Real>
+__device__ __forceinline__ void mixer_bits2(V2<Real>* S, uint32_t len, uint32_t k0, uint32_t k1, Real c, Real s) {
+  auto rx = [&](V2<Real>& a, V2<Real>& b) {
+    const V2<Real> x = a, y = b;
+    a = mk<Real>(c * x.x + s * y.y, c * x.y - s * y.x);
+    b = mk<Real>(c * y.x + s * x.y, c * y.y - s * x.x);
+  };
+  for (uint32_t i = threadIdx.x; i < len / 4; i += THREADS) {
+    const uint32_t e00 = (uint32_t)insert_zero(insert_zero(i, k0), k1);
+    const uint32_t e01 = e00 | (1u << k0), e10 = e00 | (1u << k1), e11 = e01 | (1u << k1);
+    V2<Real> a00 = S[e00], a01 = S[e01], a10 = S[e10], a11 = S[e11];
+    rx(a00, a01);
+    rx(a10, a11);
+    rx(a00, a10);
+    rx(a01, a11);
+    S[e00] = a00;
+    S[e01] = a01;
+    S[e10] = a10;
+    S[e11] = a11;
+  }
+}
+
+// Rx on the tile-local bits first, first+1, ..., first+count-1: two per sweep.
+template <typename Real>
+__device__ __forceinline__ void mixer_range(V2<Real>* S, uint32_t len, uint32_t first, uint32_t count, Real c, Real s) {
+  uint32_t k = 0;
+  for (; k + 1 < count; k += 2) {
+    __syncthreads();
+    mixer_bits2<Real>(S, len, first + k, first + k + 1, c, s);
+  }
+  if (k < count) {
+    __syncthreads();
+    mixer_bit<Real>(S, len, first + k, c, s);
+  }
+  __syncthreads();
+}
+
 __device__ __forceinline__ double block_sum(double v, double* red) {
   for (int o = 16; o; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
@@ -77,11 +119,11 @@ __device__ __forceinline__ double block_sum(double v, double* red) {
 }
 
 template <typename Real>
-__global__ void __launch_bounds__(THREADS, 1) sweep_kernel(Args a) {
+__global__ void __launch_bounds__(THREADS, Cfg<Real>::CTAS_PER_SM) sweep_kernel(Args a) {
   extern __shared__ __align__(16) uint8_t qsm[];
   V2<Real>* S = (V2<Real>*)qsm;
   __shared__ uint8_t eu[MAX_EDGES], ev[MAX_EDGES];
-  __shared__ uint8_t cutT[1 << 14];
+  __shared__ uint8_t cutT[1 << TILE_BITS];
   __shared__ uint8_t X0[128], X1[64];
   __shared__ V2<Real> ph[MAX_EDGES + 1];  // cost-layer phase by cut value
   __shared__ double red[THREADS / 32];
@@ -136,11 +178,7 @@ __global__ void __launch_bounds__(THREADS, 1) sweep_kernel(Args a) {
         for (uint32_t i = tid; i < L; i += THREADS) S[i] = cmul<Real>(ph[cutT[i]], S[i]);
         double sb, cb;
         sincos(bet[l], &sb, &cb);
-        for (uint32_t k = 0; k < n; ++k) {
-          __syncthreads();
-          mixer_bit<Real>(S, L, k, (Real)cb, (Real)sb);
-        }
-        __syncthreads();
+        mixer_range<Real>(S, L, 0, n, (Real)cb, (Real)sb);
       }
       for (uint32_t i = tid; i < L; i += THREADS) {
         const double x = (double)S[i].x, y = (double)S[i].y;
@@ -190,11 +228,7 @@ __global__ void __launch_bounds__(THREADS, 1) sweep_kernel(Args a) {
             const V2<Real> v = l == 0 ? mk<Real>(amp0, (Real)0) : X[g0 + i];
             S[i] = cmul<Real>(ph[cut], v);
           }
-          for (uint32_t k = 0; k < (uint32_t)TILE_BITS; ++k) {
-            __syncthreads();
-            mixer_bit<Real>(S, TILE, k, rc, rs);
-          }
-          __syncthreads();
+          mixer_range<Real>(S, TILE, 0, TILE_BITS, rc, rs);
           for (uint32_t i = tid; i < TILE; i += THREADS) X[g0 + i] = S[i];
           __syncthreads();
         }
@@ -206,11 +240,7 @@ __global__ void __launch_bounds__(THREADS, 1) sweep_kernel(Args a) {
             return lo | (t << c) | (hi << TILE_BITS);
           };
           for (uint32_t i = tid; i < TILE; i += THREADS) S[i] = X[gidx(i)];
-          for (uint32_t k = 0; k < h; ++k) {
-            __syncthreads();
-            mixer_bit<Real>(S, TILE, c + k, rc, rs);
-          }
-          __syncthreads();
+          mixer_range<Real>(S, TILE, c, h, rc, rs);
           if (last) {
             for (uint32_t i = tid; i < TILE; i += THREADS) {
               const double x = (double)S[i].x, y = (double)S[i].y;
@@ -233,6 +263,10 @@ __global__ void __launch_bounds__(THREADS, 1) sweep_kernel(Args a) {
 
 uint32_t qaoa_smem_max_n(int precision) {
   return precision == ALEPH_B200_F64 ? (uint32_t)qaoa::Cfg<double>::SMEM_N : (uint32_t)qaoa::Cfg<float>::SMEM_N;
+}
+
+int qaoa_ctas_per_sm(int precision) {
+  return precision == ALEPH_B200_F64 ? qaoa::Cfg<double>::CTAS_PER_SM : qaoa::Cfg<float>::CTAS_PER_SM;
 }
 
 cudaError_t launch_qaoa_sweep(int precision, const aleph_b200_qaoa_set* sets, const uint32_t* edges,

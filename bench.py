@@ -305,6 +305,132 @@ def fidelity_check(n: int, depth: int, seed: int) -> dict:
             "against": "this engine's FP64 path (held to 1e-12 of the FP64 oracle by the parity tests)"}
 
 
+def learned_choice(be, n, flat, precision):
+    """The configuration the committed cost model ranks first (None without a model)."""
+    from aleph_b200 import learned
+
+    if not learned.MODEL_PATH.exists():
+        return None
+    model = learned.CostModel.load(be, learned.MODEL_PATH)
+    try:
+        return learned.LearnedPlanner(model).score(n, flat, precision)[0].choice
+    finally:
+        model.free()
+
+
+def qaoa_sweep_bench(dev: int, sets: int, loop_sample: int, seed: int) -> dict:
+    """Batched QAOA Max-Cut sweep: `sets` parameter sets, n uniform in 12..24,
+    random 3-regular graphs (odd n: random graphs with 3n/2 edges), p = 4,
+    angles uniform in [0, pi]; FP32 and FP64 states, <C> in FP64. Compared with
+    a per-circuit launch loop through the engine's gate-stream path."""
+    from aleph_b200 import workloads
+    from aleph_b200.backend import B200SvBackend
+
+    rng = np.random.default_rng(seed)
+    graphs = []
+    for n in rng.integers(12, 25, sets):
+        n = int(n)
+        if n % 2 == 0:
+            graphs.append((n, workloads.random_3_regular(n, rng)))
+        else:
+            e = set()
+            while len(e) < (3 * n) // 2:
+                i, j = (int(x) for x in rng.choice(n, 2, replace=False))
+                e.add((min(i, j), max(i, j)))
+            graphs.append((n, sorted(e)))
+    gam = rng.uniform(0, np.pi, (sets, 4))
+    bet = rng.uniform(0, np.pi, (sets, 4))
+    out = {"sets": sets, "n_range": [12, 24], "p": 4}
+    vals = {}
+    for prec in ("f32", "f64"):
+        be = B200SvBackend(seed=0, device=dev, precision=prec)
+        be.qaoa_sweep(graphs, gam, bet)  # capture + warm-up
+        ts = []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            vals[prec] = be.qaoa_sweep(graphs, gam, bet)
+            ts.append(time.perf_counter() - t0)
+        out[f"{prec}_circuits_per_s"] = round(sets / min(ts), 1)
+        if prec == "f32":
+            t0 = time.perf_counter()
+            for k in range(loop_sample):
+                n, e = graphs[k]
+                st = be.allocate(n)
+                be.apply_stream(st, workloads.qaoa_maxcut(n, e, gam[k], bet[k]).instructions)
+                sum(0.5 * (1 - be.expectation_value(st, [(i, "Z"), (j, "Z")])) for (i, j) in e)
+                st.free()
+            per = (time.perf_counter() - t0) / loop_sample
+            out["per_circuit_loop_circuits_per_s"] = round(1.0 / per, 1)
+            out["per_circuit_loop_sample"] = loop_sample
+        be.close()
+    out["sweep_speedup_f32"] = round(out["f32_circuits_per_s"] / out["per_circuit_loop_circuits_per_s"], 1)
+    out["max_abs_c_f32_vs_f64"] = float(np.abs(vals["f32"] - vals["f64"]).max())
+    return out
+
+
+def small_configs_bench(dev: int, seed: int) -> dict:
+    """The two plain-FP64 configurations beside the headline:
+    C0: brickwall n=20 depth 20, full state and 1024 shots against the oracle;
+    C1: textbook QFT (with bit-reversal swaps) on a random Ry.Rz product state
+    at n=30: time, ||psi||^2 and 4096 shots on the device, and max|dpsi|
+    against the oracle on the n=24 copy of the circuit."""
+    import torch
+
+    from aleph_b200 import workloads
+    from aleph_b200.backend import B200SvBackend
+    from oracle import oracle
+
+    out = {}
+    be = B200SvBackend(seed=seed, device=dev, precision="f64")
+    stream = torch.cuda.ExternalStream(be.stream_ptr())
+
+    def timed(n, circ, reps=3):
+        plan = be.compile(n, circ.instructions)
+        st = be.allocate(n)
+        be.reset_state(st)
+        plan.execute(st)
+        ms = []
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            be.reset_state(st)
+            plan.execute(st)
+            e1.record(stream)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        plan.free()
+        return st, min(ms)
+
+    c0 = workloads.brickwall(20, 20, seed=seed)
+    st, ms = timed(20, c0)
+    psi = be.statevector(st)
+    want, _ = oracle.run(20, c0.instructions)
+    words = workloads.splitmix64_words(seed, 1024)
+    shots_ok = bool(np.array_equal(be.sample(st, 1024, variates=words, mode="alias"), oracle.sample_alias(want, words)))
+    out["c0_brickwall_n20_d20"] = {"ms": round(ms, 3), "max_abs_dpsi": float(np.abs(psi - want).max()),
+                                   "shots_1024_identical": shots_ok}
+    st.free()
+
+    c1 = workloads.qft_product(30, seed=seed)
+    st, ms = timed(30, c1)
+    norm = be.norm_sqr(st)
+    u = np.random.default_rng(seed).random(4096)
+    t0 = time.perf_counter()
+    be.sample(st, 4096, variates=u, mode="cumulative")
+    shots_ms = (time.perf_counter() - t0) * 1e3
+    st.free()
+    c1s = workloads.qft_product(24, seed=seed)
+    st24 = be.allocate(24)
+    be.apply_stream(st24, c1s.instructions)
+    w24, _ = oracle.run(24, c1s.instructions)
+    out["c1_qft_n30"] = {"ms": round(ms, 3), "norm_sqr": norm, "shots_4096_ms": round(shots_ms, 2),
+                         "shots_mode": "cumulative (alias tables are built up to n=28)",
+                         "n24_copy_max_abs_dpsi": float(np.abs(be.statevector(st24) - w24).max())}
+    st24.free()
+    be.close()
+    return out
+
+
 def run_engine(args, ranks: Ranks):
     import torch
 
@@ -320,8 +446,12 @@ def run_engine(args, ranks: Ranks):
     circ = workloads.brickwall(n, depth, seed=args.seed)
     flat = flatten(circ.instructions)
 
-    # -- TC-FP32, device-resident: the headline value
+    # -- TC-FP32, device-resident: the headline value, on the plan configuration
+    #    the learned cost model scores best (the greedy configuration without a model)
     be = B200SvBackend(seed=args.seed, device=dev, precision=args.precision)
+    choice = learned_choice(be, n, flat, args.precision) if not args.greedy else None
+    if choice is not None:
+        choice.apply(be)
     plan = be.compile(n, flat)
     st = be.allocate(n)
     clocks = ClockSampler(dev)
@@ -399,6 +529,13 @@ def run_engine(args, ranks: Ranks):
     if args.fidelity_n and ranks.rank == 0:
         fid = fidelity_check(args.fidelity_n, depth, args.seed)
 
+    qaoa = None
+    if args.qaoa_sets and ranks.rank == 0:
+        qaoa = qaoa_sweep_bench(dev, args.qaoa_sets, 8, args.seed)
+    small = None
+    if not args.skip_small and ranks.rank == 0:
+        small = small_configs_bench(dev, args.seed)
+
     cpu = None
     if ranks.world == 1 and not args.skip_cpu:
         cores = host_cores()
@@ -416,6 +553,8 @@ def run_engine(args, ranks: Ranks):
                            parallelism=f"replicas x{ranks.world}" if ranks.world > 1 else "single GPU"),
             "clocks": clk, "e2e": e2e, "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu,
             "kernels": table, "fp64_plain": fp64, "fidelity": fid, "final_norm_sqr": norm,
+            "plan_choice": None if choice is None else dict(choice.__dict__, source="learned cost model"),
+            "qaoa_sweep": qaoa, "fp64_configs": small,
         }
         print(json.dumps(line), flush=True)
     ranks.close()
@@ -423,9 +562,14 @@ def run_engine(args, ranks: Ranks):
 
 
 # DRAM bytes (read + write) per amplitude of one launch of the dominant
-# kernel, from an ncu capture of that kernel on a smaller register, scaled by
-# the amplitudes it processes (traffic grows in proportion to 2^n).
-TRAFFIC_PER_AMP: dict[tuple[str, str], float] = {}
+# kernel, from an ncu capture of that kernel on a smaller register (n=26),
+# scaled by the amplitudes it processes (traffic grows in proportion to 2^n):
+# block_kernel 537.0 MB read + 479.2 MB written over 2^26 amplitudes;
+# tile_kernel (FP64) 1.074 GB + 1.068 GB over 2^26.
+TRAFFIC_PER_AMP: dict[tuple[str, str], float] = {
+    ("tc32", "block"): (537.031936e6 + 479.182848e6) / 2**26,
+    ("f64", "tile"): (1.074011e9 + 1.067877e9) / 2**26,
+}
 
 
 def main(argv=None):
@@ -446,6 +590,9 @@ def main(argv=None):
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--cpu-sample-n", type=int, default=26)
     ap.add_argument("--ref-sample-n", type=int, default=26)
+    ap.add_argument("--qaoa-sets", type=int, default=4096, help="QAOA sweep size (0: skip)")
+    ap.add_argument("--greedy", action="store_true", help="the greedy plan configuration, no cost model")
+    ap.add_argument("--skip-small", action="store_true", help="skip the n=20 brickwall / n=30 QFT FP64 checks")
     args = ap.parse_args(argv)
     args.warmup = max(3, args.warmup)  # at least 3 untimed warm-up steps
     ranks = Ranks()
