@@ -52,12 +52,15 @@ namespace ab {
 
 namespace blk {
 
-constexpr int CONV_WARP0 = 0;   // warps 0..7: two per TMEM lane quarter, one per half of the block rows
-constexpr int EPI_WARP0 = 8;    // warps 8..15: same split
-constexpr int TMA_WARP = 16;
-constexpr int MMA_WARP = 17;
-constexpr int THREADS = 18 * 32;
-constexpr int ROLE_WARPS = 8;   // converter / epilogue warps (mbarrier arrival counts)
+constexpr int CONV_WARP0 = 0;   // warps 0..3: one per TMEM lane quarter, all 64 block rows
+constexpr int CONV_WARPS = 4;
+constexpr int EPI_WARP0 = 4;    // warps 4..11: two per TMEM lane quarter, one per half of the block rows
+constexpr int EPI_WARPS = 8;
+constexpr int TMA_WARP = 12;
+constexpr int MMA_WARP = 13;
+// 14 warps: with per-SMSP warp slots allocated four at a time this leaves
+// 128 registers per thread (18 warps would cap them at 96 and spill)
+constexpr int THREADS = 14 * 32;
 constexpr int NCOL = 128;                     // columns per tile (MMA M)
 constexpr int TILE_AMPS = 64 * NCOL;          // 8192 complex
 constexpr int TILE_BYTES = TILE_AMPS * 8;     // 64 KiB FP32 complex
@@ -265,11 +268,11 @@ __global__ void __launch_bounds__(blk::THREADS, 1) block_kernel(const __grid_con
     mbar_init(bar_w, 1);
     for (int b = 0; b < 2; ++b) {
       mbar_init(bar_sfull + 8 * b, 1);
-      mbar_init(bar_sempty + 8 * b, ROLE_WARPS);
-      mbar_init(bar_afull + 8 * b, ROLE_WARPS);
+      mbar_init(bar_sempty + 8 * b, CONV_WARPS);
+      mbar_init(bar_afull + 8 * b, CONV_WARPS);
       mbar_init(bar_aempty + 8 * b, 1);
       mbar_init(bar_dfull + 8 * b, 1);
-      mbar_init(bar_dempty + 8 * b, ROLE_WARPS);
+      mbar_init(bar_dempty + 8 * b, EPI_WARPS);
     }
     fence_barrier_init();
     abort_sh = 0;
@@ -339,7 +342,6 @@ __global__ void __launch_bounds__(blk::THREADS, 1) block_kernel(const __grid_con
   } else if (warp < EPI_WARP0) {
     // ---------------- converters: stage -> BF16 hi/lo -> TMEM A operand ----------------
     const int q = warp & 3;  // TMEM lane quarter
-    const int h = (warp - CONV_WARP0) >> 2;  // block rows 32h .. 32h+31
     const int col = 32 * q + lane;
     const uint32_t lc = Lcol[col];
     uint32_t i = 0;
@@ -352,7 +354,8 @@ __global__ void __launch_bounds__(blk::THREADS, 1) block_kernel(const __grid_con
       tc_fence_after();
       const uint8_t* stg = sm + OFF_S + s * STAGE_BYTES + lc;  // this thread's column
       const uint32_t ta = tmem + TM_A + 128 * s + ((uint32_t)(32 * q) << 16);  // this warp's lanes
-      {
+#pragma unroll 1
+      for (int h = 0; h < 2; ++h) {  // block rows 32h .. 32h+31
         uint32_t hr[16], hi[16], lr[16], li[16];
 #pragma unroll
         for (int p = 0; p < 16; ++p) {
