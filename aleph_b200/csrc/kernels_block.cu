@@ -13,20 +13,21 @@
 // accumulated in FP32 in TMEM: ~16 significant bits per operand at three BF16
 // MMAs per product.
 //
-// Warp-specialised persistent kernel, one CTA per SM, 18 warps:
-//   * warp 16 (TMA): fetches each tile (64 block rows x 128 columns = 64 KiB
+// Warp-specialised persistent kernel, one CTA per SM, 14 warps:
+//   * warp 12 (TMA): fetches each tile (64 block rows x 128 columns = 64 KiB
 //     FP32) with plain (non-multicast) cp.async.bulk copies of its contiguous
 //     runs into one of two shared-memory stages (mbarrier transaction counts);
-//   * warps 0-7 (converters): thread c takes column c of the staged tile (one
-//     half of its block rows per warp group), splits the real values into
-//     BF16 hi/lo and writes them with tcgen05.st into TMEM lane c: the A
-//     operand of the MMA lives in tensor memory (two buffers), so shared
-//     memory only holds W and the stages;
-//   * warp 17 (one thread): issues 3 x 8 tcgen05.mma (A from TMEM, M=128
+//   * warps 0-3 (converters): thread c takes column c of the staged tile (all
+//     64 block rows), splits the real values into BF16 hi/lo and writes them
+//     with tcgen05.st into TMEM lane c: the A operand of the MMA lives in
+//     tensor memory (two buffers), so shared memory only holds W and the
+//     stages;
+//   * warp 13 (one thread): issues 3 x 8 tcgen05.mma (A from TMEM, M=128
 //     columns; B = W_hi / W_lo from shared memory, N=128, K=16; kind::f16,
 //     BF16 in, FP32 accumulate) into one of two TMEM accumulators and commits
 //     to mbarriers that free the A buffer and hand the accumulator over;
-//   * warps 8-15 (epilogue): tcgen05.ld the accumulator (32x32b: one column
+//   * warps 4-11 (epilogue, two per TMEM lane quarter, one per half of the
+//     block rows): tcgen05.ld the accumulator (32x32b: one column
 //     per thread), apply the diagonal ops that follow the block (CZ-like sign
 //     flips as one 64-bit row mask per thread, other phases per element) and
 //     store straight to HBM (16-byte stores of row pairs when the block holds
