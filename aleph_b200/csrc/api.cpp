@@ -393,6 +393,7 @@ int aleph_b200_destroy(aleph_b200_handle* h) {
   if (h->stream) cudaStreamSynchronize(h->stream);
   for (Scratch* s : {&h->reduce, &h->plan_buf, &h->sample, &h->status, &h->qaoa.dev, &h->qaoa.state, &h->qaoa.cuts})
     if (s->ptr) cudaFree(s->ptr);
+  for (Scratch& s : h->state_pool) cudaFree(s.ptr);
   if (h->qaoa.exec) cudaGraphExecDestroy(h->qaoa.exec);
   if (h->qaoa.host_in) cudaFreeHost(h->qaoa.host_in);
   if (h->qaoa.host_out) cudaFreeHost(h->qaoa.host_out);
@@ -424,7 +425,24 @@ int aleph_b200_allocate(aleph_b200_handle* h, uint32_t n, aleph_b200_state** out
   st->n = n;
   st->precision = h->precision == ALEPH_B200_F64 ? ALEPH_B200_F64 : ALEPH_B200_F32;
   st->bytes = (size_t)(st->precision == ALEPH_B200_F64 ? 16 : 8) << n;
-  cudaError_t e = cudaMalloc(&st->amps, st->bytes);
+  st->amps = nullptr;
+  for (size_t k = 0; k < h->state_pool.size(); ++k)
+    if (h->state_pool[k].bytes == st->bytes) {  // a freed buffer of this size: reuse it, in stream order
+      st->amps = h->state_pool[k].ptr;
+      h->state_pool.erase(h->state_pool.begin() + (long)k);
+      break;
+    }
+  cudaError_t e = cudaSuccess;
+  if (!st->amps) {
+    e = cudaMalloc(&st->amps, st->bytes);
+    if (e == cudaErrorMemoryAllocation && !h->state_pool.empty()) {  // give the pooled buffers back, retry
+      cudaGetLastError();
+      cudaStreamSynchronize(h->stream);
+      for (Scratch& s : h->state_pool) cudaFree(s.ptr);
+      h->state_pool.clear();
+      e = cudaMalloc(&st->amps, st->bytes);
+    }
+  }
   if (e != cudaSuccess) {
     delete st;
     cudaGetLastError();
@@ -441,13 +459,25 @@ int aleph_b200_allocate(aleph_b200_handle* h, uint32_t n, aleph_b200_state** out
   return ALEPH_B200_OK;
 }
 
+// With a handle, the buffer goes to the handle's pool (at most two are kept;
+// an older one is released): later kernels on the handle's stream are
+// ordered after the ones that used it, so no synchronisation is needed.
 int aleph_b200_free_state(aleph_b200_handle* h, aleph_b200_state* st) {
   if (!st) return ALEPH_B200_OK;
   if (h) {
     cudaSetDevice(h->device);
-    cudaStreamSynchronize(h->stream);
+    if (h->state_pool.size() >= 2) {
+      cudaStreamSynchronize(h->stream);
+      cudaFree(h->state_pool.front().ptr);
+      h->state_pool.erase(h->state_pool.begin());
+    }
+    Scratch s;
+    s.ptr = st->amps;
+    s.bytes = st->bytes;
+    h->state_pool.push_back(s);
+  } else {
+    cudaFree(st->amps);
   }
-  cudaFree(st->amps);
   delete st;
   return ALEPH_B200_OK;
 }

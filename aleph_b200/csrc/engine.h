@@ -156,6 +156,9 @@ struct Handle {
   Scratch plan_buf;  // uploaded plan tables
   Scratch sample;    // sampling tables
   Scratch status;    // device status words (measure outcomes, error flags)
+  // freed state buffers kept for reuse by the next allocate of the same size
+  // (stream-ordered: reuse runs after the kernels that used the buffer)
+  std::vector<Scratch> state_pool;
   // per-pass timing (record_passes)
   bool record_passes = false;
   std::vector<cudaEvent_t> events;

@@ -20,6 +20,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <thread>
 
 #include "engine.h"
 
@@ -740,9 +741,58 @@ void block_take(const std::vector<const Lowered*>& pending, uint64_t fixedB, boo
   out->B = B;
 }
 
+// One block pass's fused unitary, still to be built: its ops, its qubits and
+// the byte offset of its image in the plan.
+struct BlockJob {
+  std::vector<const Lowered*> take;
+  uint32_t bq[6];
+  uint32_t mat;
+};
+
+// Fuse each job's ops into a 64x64 unitary (columns = images of the basis
+// vectors, in FP64), lay it out as W = [[Re U, -Im U], [Im U, Re U]] and write
+// the split-BF16 image. The jobs are independent: they run on host threads.
+void build_block_images(const std::vector<BlockJob>& jobs, Plan* P) {
+  if (jobs.empty()) return;
+  P->block_images.resize(P->block_images.size() + jobs.size() * kBlockImageBytes);
+  auto build = [&](size_t k) {
+    const BlockJob& J = jobs[k];
+    std::vector<Cx> U(64 * 64);
+    for (uint32_t col = 0; col < 64; ++col) {
+      Cx s[64];
+      for (uint32_t x = 0; x < 64; ++x) s[x] = Cx{x == col ? 1.0 : 0.0, 0.0};
+      for (const Lowered* L : J.take) apply_local(*L, J.bq, s);
+      for (uint32_t x = 0; x < 64; ++x) U[x * 64 + col] = s[x];
+    }
+    std::vector<double> W(128 * 128);
+    for (uint32_t r = 0; r < 64; ++r)
+      for (uint32_t c = 0; c < 64; ++c) {
+        const Cx u = U[r * 64 + c];
+        W[r * 128 + c] = u.re;
+        W[r * 128 + 64 + c] = -u.im;
+        W[(64 + r) * 128 + c] = u.im;
+        W[(64 + r) * 128 + 64 + c] = u.re;
+      }
+    build_block_image(W.data(), P->block_images.data() + J.mat);
+  };
+  const unsigned hw = std::thread::hardware_concurrency();
+  const size_t nt = std::min<size_t>(jobs.size(), hw ? std::min(hw, 16u) : 1u);
+  if (nt <= 1) {
+    for (size_t k = 0; k < jobs.size(); ++k) build(k);
+    return;
+  }
+  std::vector<std::thread> ws;
+  for (size_t t = 0; t < nt; ++t)
+    ws.emplace_back([&, t] {
+      for (size_t k = t; k < jobs.size(); k += nt) build(k);
+    });
+  for (auto& w : ws) w.join();
+}
+
 int plan_segment_blocks(const std::vector<const Lowered*>& seg, uint32_t n, uint32_t R, bool window_search,
                         Plan* P) {
   std::vector<const Lowered*> pending = seg;
+  std::vector<BlockJob> jobs;
   while (!pending.empty()) {
     // Candidates: the first-come block, and (window_search) every window of 6
     // consecutive qubits; the one that consumes the most ops wins (ties keep
@@ -772,30 +822,12 @@ int plan_segment_blocks(const std::vector<const Lowered*>& seg, uint32_t n, uint
     uint32_t bq[6], nb = 0;
     for (uint32_t q = 0; q < n; ++q)
       if ((B >> q) & 1) bq[nb++] = q;
-    // fused unitary, columns = images of the basis vectors
-    std::vector<Cx> U(64 * 64);
-    for (uint32_t col = 0; col < 64; ++col) {
-      Cx s[64];
-      for (uint32_t x = 0; x < 64; ++x) s[x] = Cx{x == col ? 1.0 : 0.0, 0.0};
-      for (const Lowered* L : take) apply_local(*L, bq, s);
-      for (uint32_t x = 0; x < 64; ++x) U[x * 64 + col] = s[x];
-    }
-    std::vector<double> W(128 * 128);
-    for (uint32_t r = 0; r < 64; ++r)
-      for (uint32_t k = 0; k < 64; ++k) {
-        const Cx u = U[r * 64 + k];
-        W[r * 128 + k] = u.re;
-        W[r * 128 + 64 + k] = -u.im;
-        W[(64 + r) * 128 + k] = u.im;
-        W[(64 + r) * 128 + 64 + k] = u.re;
-      }
     Pass ps{};
     ps.kind = PASS_BLOCK;
     ps.block.n = n;
     for (int j = 0; j < 6; ++j) ps.block.bq[j] = bq[j];
-    ps.block.mat = (uint32_t)P->block_images.size();
-    P->block_images.resize(P->block_images.size() + kBlockImageBytes);
-    build_block_image(W.data(), P->block_images.data() + ps.block.mat);
+    ps.block.mat = (uint32_t)(P->block_images.size() + jobs.size() * kBlockImageBytes);
+    jobs.push_back(BlockJob{take, {bq[0], bq[1], bq[2], bq[3], bq[4], bq[5]}, ps.block.mat});
     ps.block.post_begin = (uint32_t)P->ops.size();
     for (const Lowered* L : post) append_op(P, *L, L->op);
     ps.block.post_count = (uint32_t)P->ops.size() - ps.block.post_begin;
@@ -807,6 +839,7 @@ int plan_segment_blocks(const std::vector<const Lowered*>& seg, uint32_t n, uint
     P->passes.push_back(ps);
     pending.swap(rest);
   }
+  build_block_images(jobs, P);
   return ALEPH_B200_OK;
 }
 
