@@ -141,22 +141,32 @@ class ClockSampler:
 
 # ---- distributed plumbing (replicas only) -------------------------------------
 class Ranks:
+    """One process per GPU (torchrun's RANK / LOCAL_RANK / WORLD_SIZE). The
+    replicas share no data: the process group carries only the barriers
+    around the timed region and the max-over-ranks of the times (NCCL on
+    GPUs, gloo on CPU-only hosts)."""
+
     def __init__(self):
         self.world = int(os.environ.get("WORLD_SIZE", "1"))
         self.rank = int(os.environ.get("RANK", "0"))
         self.local = int(os.environ.get("LOCAL_RANK", "0"))
         self.pg = False
+        self.cuda = False
 
-    def init(self):
+    def init(self, timeout_s: int = 600):
         if self.world > 1:
             import datetime
 
             import torch
             import torch.distributed as dist
 
-            torch.cuda.set_device(self.local)
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
-                                    device_id=torch.device("cuda", self.local))
+            self.cuda = torch.cuda.is_available()
+            if self.cuda:
+                torch.cuda.set_device(self.local)
+                dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=timeout_s),
+                                        device_id=torch.device("cuda", self.local))
+            else:
+                dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=timeout_s))
             self.pg = True
 
     def barrier(self):
@@ -171,7 +181,7 @@ class Ranks:
         import torch
         import torch.distributed as dist
 
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{self.local}")
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{self.local}" if self.cuda else "cpu")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
