@@ -40,6 +40,17 @@ template <typename Real, int R, int J>
 __device__ __forceinline__ void reg_1q(V2<Real> (&v)[1 << R], const V2<Real>* m, bool thr, uint32_t creg) {
   const V2<Real> m0 = ld_coef<Real>(m), m1 = ld_coef<Real>(m + 1), m2 = ld_coef<Real>(m + 2),
                  m3 = ld_coef<Real>(m + 3);
+  if (thr && creg == 0) {  // no register-part controls: every pair, no per-pair predicate
+#pragma unroll
+    for (int r = 0; r < (1 << R); ++r) {
+      if (r & (1 << J)) continue;
+      const int r1 = r | (1 << J);
+      const V2<Real> a = v[r], b = v[r1];
+      v[r] = cmul2<Real>(m0, a, m1, b);
+      v[r1] = cmul2<Real>(m2, a, m3, b);
+    }
+    return;
+  }
 #pragma unroll
   for (int r = 0; r < (1 << R); ++r) {
     if (r & (1 << J)) continue;
@@ -90,6 +101,14 @@ __device__ __forceinline__ void lane_1q(V2<Real> (&v)[1 << R], int s, const V2<R
   const bool hi = (lane >> s) & 1;
   const V2<Real> cs = ld_coef<Real>(m + (hi ? 3 : 0));  // coefficient on own amplitude
   const V2<Real> co = ld_coef<Real>(m + (hi ? 2 : 1));  // coefficient on partner amplitude
+  if (thr && creg == 0) {  // no register-part controls
+#pragma unroll
+    for (int r = 0; r < (1 << R); ++r) {
+      const V2<Real> o = shfl_xor<Real>(v[r], 1 << s);
+      v[r] = cmul2<Real>(cs, v[r], co, o);
+    }
+    return;
+  }
 #pragma unroll
   for (int r = 0; r < (1 << R); ++r) {
     const V2<Real> o = shfl_xor<Real>(v[r], 1 << s);
