@@ -15,7 +15,10 @@
 // 2^13 amplitudes, two passes per layer: pass A over contiguous chunks
 // (qubits 0..12: cost phase + mixer), pass B over tiles spanning the qubits
 // 13..n-1 (mixer). The first pass generates |+>^n instead of reading it; the
-// last pass only reads and accumulates <C>.
+// last pass only reads and accumulates <C>. A pass loads a tile into
+// registers (32 amplitudes a thread, every load in flight at once), mixes the
+// register and lane bits there, and at most one trip through shared memory
+// mixes the warp bits.
 //
 // cut(z) per amplitude: within a pass-A chunk z = (t << 13) | lo and
 // cut(z) = cutT[lo] + (edges among the high qubits cut by t) + X0[lo & 127] +
@@ -107,6 +110,66 @@ __device__ __forceinline__ void mixer_range(V2<Real>* S, uint32_t len, uint32_t 
   __syncthreads();
 }
 
+// Streamed tiles are swept in registers. Register layout: tile index
+// i = tid | r << 8 (lane = tile bits 0..4, warp = bits 5..7, register r =
+// bits 8..12), so one thread issues all REGS of its loads before it uses one.
+constexpr int REGS = TILE / THREADS;
+static_assert(THREADS == 256 && REGS == 32, "the sweep layouts assume 8 warps and 32 registers");
+
+template <typename Real>
+__device__ __forceinline__ void rx_pair(V2<Real>& a, V2<Real>& b, Real c, Real s) {
+  const V2<Real> x = a, y = b;
+  a = mk<Real>(c * x.x + s * y.y, c * x.y - s * y.x);
+  b = mk<Real>(c * y.x + s * x.y, c * y.y - s * x.x);
+}
+
+// Rx(2 beta) on register bit k of v for every k set in mask.
+template <typename Real, int NR>
+__device__ __forceinline__ void rx_regs(V2<Real> (&v)[NR], uint32_t mask, Real c, Real s) {
+#pragma unroll
+  for (int k = 0; (1 << k) < NR; ++k) {
+    if (!((mask >> k) & 1u)) continue;
+#pragma unroll
+    for (int r = 0; r < NR; ++r)
+      if (!(r & (1 << k))) rx_pair<Real>(v[r], v[r | (1 << k)], c, s);
+  }
+}
+
+// Rx(2 beta) on lane bit k for every k set in mask (uniform across the warp):
+// the partner amplitude comes from lane ^ (1 << k), and both halves of a pair
+// take the same form x' = c x - i s y.
+template <typename Real, int NR>
+__device__ __forceinline__ void rx_lanes(V2<Real> (&v)[NR], uint32_t mask, Real c, Real s) {
+#pragma unroll
+  for (int k = 0; k < 5; ++k) {
+    if (!((mask >> k) & 1u)) continue;
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+      const Real yx = __shfl_xor_sync(0xffffffffu, v[r].x, 1 << k);
+      const Real yy = __shfl_xor_sync(0xffffffffu, v[r].y, 1 << k);
+      v[r] = mk<Real>(c * v[r].x + s * yy, c * v[r].y - s * yx);
+    }
+  }
+}
+
+// One read of the tile in shared memory in the layout lane = tile bits 0..4,
+// register = bits 5..7, warp and loop = bits 8..12: Rx on the register bits
+// set in mask3, then emit(i, amplitude) for each of this thread's 32 indices.
+template <typename Real, typename Emit>
+__device__ __forceinline__ void shared_sweep(const V2<Real>* S, uint32_t mask3, Real c, Real s, Emit&& emit) {
+  const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const uint32_t hi = (w | (uint32_t)j << 3) << 8;
+    V2<Real> u[8];
+#pragma unroll
+    for (int r = 0; r < 8; ++r) u[r] = S[hi | (uint32_t)r << 5 | lane];
+    rx_regs<Real, 8>(u, mask3, c, s);
+#pragma unroll
+    for (int r = 0; r < 8; ++r) emit(hi | (uint32_t)r << 5 | lane, u[r]);
+  }
+}
+
 __device__ __forceinline__ double block_sum(double v, double* red) {
   for (int o = 16; o; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
@@ -186,17 +249,19 @@ __global__ void __launch_bounds__(THREADS, Cfg<Real>::CTAS_PER_SM) sweep_kernel(
       }
     } else {
       // ---- streamed through this CTA's state slice ----
-      const uint32_t h = n - TILE_BITS;     // qubits 13..n-1
-      const uint32_t c = TILE_BITS - h;     // pass B: low run bits (n <= 26)
+      const uint32_t c = 2 * TILE_BITS - n;                 // pass B: low run bits (n <= 26)
+      const uint32_t maskB = (TILE - 1) & ~((1u << c) - 1);  // pass B mixes tile bits c..12
       const uint64_t ntiles = len >> TILE_BITS;
+      V2<Real> v[REGS];  // the register sweep's amplitudes (see load_chunk / load_tile)
       for (uint32_t l = 0; l < a.p; ++l) {
         set_phases(gam[l]);
         double sb, cb;
         sincos(bet[l], &sb, &cb);
         const Real rc = (Real)cb, rs = (Real)sb;
-        // pass A: contiguous chunks, cost phase + mixer on qubits 0..12
-        for (uint64_t t = 0; t < ntiles; ++t) {
-          // chunk constants: cut edges among the high qubits, and the low/high cross-edge tables
+        // pass A: contiguous chunks, cost phase + mixer on qubits 0..12.
+        // Chunk constants: cut edges among the high qubits, and the low/high
+        // cross-edge tables.
+        auto chunk_tables = [&](uint32_t t) {
           if (tid == 0) {
             uint32_t ch = 0;
             for (uint32_t e = 0; e < m; ++e)
@@ -219,37 +284,74 @@ __global__ void __launch_bounds__(THREADS, Cfg<Real>::CTAS_PER_SM) sweep_kernel(
             if (tid < 128) X0[v] = (uint8_t)x;
             else X1[v] = (uint8_t)x;
           }
-          __syncthreads();
-          const uint32_t ch = s_ch;
-          const uint64_t g0 = t << TILE_BITS;
-          for (uint32_t i = tid; i < TILE; i += THREADS) {
-            const uint32_t cut = cutT[i] + ch + X0[i & 127] + X1[i >> 7];
-            if (l == 0) CG[g0 + i] = (uint8_t)cut;
-            const V2<Real> v = l == 0 ? mk<Real>(amp0, (Real)0) : X[g0 + i];
-            S[i] = cmul<Real>(ph[cut], v);
+        };
+        // this thread's 32 amplitudes i = tid | r << 8 of chunk t, every load in flight at once
+        // (slice offsets fit in 32 bits: n <= 26)
+        auto load_chunk = [&](uint32_t t) {
+          if (l == 0) {
+#pragma unroll
+            for (int r = 0; r < REGS; ++r) v[r] = mk<Real>(amp0, (Real)0);
+          } else {
+#pragma unroll
+            for (int r = 0; r < REGS; ++r) v[r] = X[(t << TILE_BITS) | tid | (uint32_t)r << 8];
           }
-          mixer_range<Real>(S, TILE, 0, TILE_BITS, rc, rs);
-          for (uint32_t i = tid; i < TILE; i += THREADS) X[g0 + i] = S[i];
+        };
+        // Software pipeline: chunk t+1's loads and tables are issued once chunk
+        // t sits in shared memory, and are in flight during its shared sweep.
+        chunk_tables(0);
+        load_chunk(0);
+        for (uint32_t t = 0; t < (uint32_t)ntiles; ++t) {
+          __syncthreads();  // chunk t's tables are visible; chunk t-1's shared sweep is done
+          const uint32_t ch = s_ch;
+          const uint32_t g0 = t << TILE_BITS;
+          const uint32_t x0 = X0[tid & 127];
+#pragma unroll
+          for (int r = 0; r < REGS; ++r) {
+            const uint32_t i = tid | (uint32_t)r << 8;
+            const uint32_t cut = cutT[i] + ch + x0 + X1[i >> 7];
+            if (l == 0) CG[g0 + i] = (uint8_t)cut;
+            v[r] = cmul<Real>(ph[cut], v[r]);
+          }
+          rx_regs<Real, REGS>(v, 0x1fu, rc, rs);   // tile bits 8..12
+          rx_lanes<Real, REGS>(v, 0x1fu, rc, rs);  // tile bits 0..4
+#pragma unroll
+          for (int r = 0; r < REGS; ++r) S[tid | (uint32_t)r << 8] = v[r];
           __syncthreads();
+          if (t + 1 < (uint32_t)ntiles) {
+            chunk_tables(t + 1);
+            load_chunk(t + 1);
+          }
+          // shared-memory sweep: tile bits 5..7, straight back to the chunk
+          shared_sweep<Real>(S, 0x7u, rc, rs, [&](uint32_t i, const V2<Real>& u) { X[g0 + i] = u; });
         }
+        __syncthreads();  // pass A's stores are visible to every thread of the CTA
         // pass B: tiles over {qubits 0..c-1} + {qubits 13..n-1}; tile index -> qubits c..12
         const bool last = l + 1 == a.p;
-        for (uint64_t t = 0; t < ntiles; ++t) {
-          auto gidx = [&](uint32_t i) -> uint64_t {
-            const uint64_t lo = i & ((1u << c) - 1), hi = i >> c;
-            return lo | (t << c) | (hi << TILE_BITS);
-          };
-          for (uint32_t i = tid; i < TILE; i += THREADS) S[i] = X[gidx(i)];
-          mixer_range<Real>(S, TILE, c, h, rc, rs);
-          if (last) {
-            for (uint32_t i = tid; i < TILE; i += THREADS) {
-              const double x = (double)S[i].x, y = (double)S[i].y;
-              acc += (x * x + y * y) * (double)CG[gidx(i)];
-            }
-          } else {
-            for (uint32_t i = tid; i < TILE; i += THREADS) X[gidx(i)] = S[i];
-          }
+        const uint32_t lowm = (1u << c) - 1;
+        auto gidx = [&](uint32_t t, uint32_t i) -> uint32_t {
+          return (i & lowm) | t << c | (i >> c) << TILE_BITS;
+        };
+        auto load_tile = [&](uint32_t t) {
+#pragma unroll
+          for (int r = 0; r < REGS; ++r) v[r] = X[gidx(t, tid | (uint32_t)r << 8)];
+        };
+        load_tile(0);
+        for (uint32_t t = 0; t < (uint32_t)ntiles; ++t) {
+          rx_regs<Real, REGS>(v, maskB >> 8, rc, rs);
+          rx_lanes<Real, REGS>(v, maskB & 0x1fu, rc, rs);
+          __syncthreads();  // the previous tile's shared-memory sweep is done
+#pragma unroll
+          for (int r = 0; r < REGS; ++r) S[tid | (uint32_t)r << 8] = v[r];
           __syncthreads();
+          if (t + 1 < (uint32_t)ntiles) load_tile(t + 1);
+          shared_sweep<Real>(S, (maskB >> 5) & 0x7u, rc, rs, [&](uint32_t i, const V2<Real>& u) {
+            if (last) {
+              const double x = (double)u.x, y = (double)u.y;
+              acc += (x * x + y * y) * (double)CG[gidx(t, i)];
+            } else {
+              X[gidx(t, i)] = u;
+            }
+          });
         }
       }
     }
