@@ -158,10 +158,11 @@ class PlanConfig(ct.Structure):
         ("smem_max_n", ct.c_uint32),
         ("block_window_search", ct.c_uint32),
         ("tile_occupancy", ct.c_uint32),
+        ("keep_swaps", ct.c_uint32),
     ]
 
 
-PASS_KINDS = {1: "tile", 2: "smem", 3: "kq", 4: "measure", 5: "block", 6: "renorm"}
+PASS_KINDS = {1: "tile", 2: "smem", 3: "kq", 4: "measure", 5: "block", 6: "renorm", 7: "permute"}
 
 # Every symbol include/aleph_b200.h declares, with its ctypes signature.
 _P = ct.c_void_p

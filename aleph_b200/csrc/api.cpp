@@ -295,6 +295,11 @@ int execute(aleph_b200_handle* h, aleph_b200_state* st, const Plan& P, const dou
         h->stats.passes++;
         h->stats.algorithmic_bytes += 2 * len * bpa;
         break;
+      case PASS_PERMUTE:
+        e = launch_permute_pass(st->amps, st->precision, st->n, ps.sigma, h->sm_count, h->stream);
+        h->stats.passes++;
+        h->stats.algorithmic_bytes += 2 * len * bpa;
+        break;
     }
     if (e != cudaSuccess) return cuda_fail(h, e, "kernel launch");
     h->stats.kernel_launches++;
@@ -509,19 +514,67 @@ int aleph_b200_apply_gate(aleph_b200_handle* h, aleph_b200_state* st, const alep
   std::vector<Lowered> ops(1);
   aleph_b200_error_info e{};
   if (lower_gate(*g, st->n, pool, pool_len, &ops[0], &e)) return report(h, e);
+  const uint32_t n = st->n;
+  if (g->kind == ALEPH_GATE_SWAP && g->num_controls == 0 && h->opts.relabel_swaps && n > h->opts.smem_max_n &&
+      n >= 6 && n <= kMaxQubits) {
+    // a SWAP of a streamed state is a permutation pass (no arithmetic; tiles
+    // that the swap leaves in place are not touched)
+    Lowered L;
+    std::memset(&L.op, 0, sizeof(Op));
+    L.is_permute = true;
+    L.sigma.resize(n);
+    for (uint32_t q = 0; q < n; ++q) L.sigma[q] = (uint8_t)q;
+    std::swap(L.sigma[g->qubits[0]], L.sigma[g->qubits[1]]);
+    L.gates = 1;
+    ops[0] = std::move(L);
+  }
   Plan P;
-  if (int s = build_plan(ops, st->n, h->opts, &P)) return set_error(h, s, "optimization pipeline failed: planner");
+  if (int s = build_plan(ops, n, h->opts, &P)) return set_error(h, s, "optimization pipeline failed: planner");
   return execute(h, st, P, nullptr, 0, nullptr, nullptr);
+}
+
+// Appends the permutation passes that move logical qubit q from position
+// phys[q] back to q (psi'(j) = psi(pi(j)), pi = phys), then resets phys.
+static void settle_relabeling(std::vector<uint32_t>& phys, uint32_t& swaps, uint32_t record, std::vector<Lowered>& ops) {
+  bool first = true;
+  for (auto& sigma : split_into_involutions(phys)) {
+    ops.emplace_back();
+    Lowered& L = ops.back();
+    std::memset(&L.op, 0, sizeof(Op));
+    L.is_permute = true;
+    L.sigma = std::move(sigma);
+    L.record = record;
+    L.gates = first ? swaps : 0;
+    first = false;
+  }
+  for (uint32_t q = 0; q < (uint32_t)phys.size(); ++q) phys[q] = q;
+  swaps = 0;
 }
 
 // Lowers a record stream for an n-qubit register into planner ops, validating
 // every record first (crates/aleph-sv/src/backend.rs apply_gate order).
+//
+// With relabel_swaps, an uncontrolled SWAP moves no data: it exchanges two
+// entries of the logical -> physical map `phys`, later records act on the
+// mapped qubits, and the map is settled by at most two in-place permutation
+// passes before a DiagonalPhase record and at the end of the stream. Errors
+// still name the logical qubits of the record as written.
 static int lower_stream(aleph_b200_handle* h, uint32_t n, const aleph_b200_instr* in, uint64_t count,
                         const aleph_b200_pools* pools, std::vector<Lowered>* out) {
   const double* pool = pools ? pools->matrix_pool : nullptr;
   const uint64_t pool_len = pools ? pools->matrix_pool_len : 0;
   std::vector<Lowered>& ops = *out;
   ops.reserve(count);
+  // states that live in shared memory for a whole pass swap qubits for free
+  const bool relabel = h->opts.relabel_swaps && n > h->opts.smem_max_n && n >= 6 && n <= kMaxQubits;
+  std::vector<uint32_t> phys(n);
+  for (uint32_t q = 0; q < n; ++q) phys[q] = q;
+  uint32_t swaps = 0;  // SWAP records absorbed since the map was last settled
+  auto mapped = [&]() {
+    for (uint32_t q = 0; q < n; ++q)
+      if (phys[q] != q) return true;
+    return false;
+  };
   for (uint64_t i = 0; i < count; ++i) {
     const aleph_b200_instr& g = in[i];
     aleph_b200_error_info e{};
@@ -530,6 +583,20 @@ static int lower_stream(aleph_b200_handle* h, uint32_t n, const aleph_b200_instr
       ops.emplace_back();
       if (lower_gate(g, n, pool, pool_len, &ops.back(), &e)) return report(h, e);
       ops.back().record = (uint32_t)i;
+      if (relabel && g.kind == ALEPH_GATE_SWAP && g.num_controls == 0) {
+        ops.pop_back();  // validated; the swap becomes a relabeling
+        std::swap(phys[g.qubits[0]], phys[g.qubits[1]]);
+        ++swaps;
+        continue;
+      }
+      if (relabel && swaps && mapped()) {
+        aleph_b200_instr gm = g;  // the same gate on the physical positions
+        for (uint32_t k = 0; k < g.num_qubits && k < 8; ++k) gm.qubits[k] = phys[g.qubits[k]];
+        for (uint32_t k = 0; k < g.num_controls && k < 8; ++k) gm.controls[k] = phys[g.controls[k]];
+        ops.back() = Lowered{};
+        if (lower_gate(gm, n, pool, pool_len, &ops.back(), &e)) return report(h, e);
+        ops.back().record = (uint32_t)i;
+      }
     } else if (g.kind == ALEPH_INSTR_MEASURE) {
       if (g.num_qubits != 1) {
         e.status = ALEPH_B200_INVALID_ARGUMENT;
@@ -545,7 +612,7 @@ static int lower_stream(aleph_b200_handle* h, uint32_t n, const aleph_b200_instr
       ops.emplace_back();
       std::memset(&ops.back().op, 0, sizeof(Op));
       ops.back().is_measure = true;
-      ops.back().measure_qubit = g.qubits[0];
+      ops.back().measure_qubit = relabel ? phys[g.qubits[0]] : g.qubits[0];
       ops.back().record = (uint32_t)i;
     } else if (g.kind == ALEPH_INSTR_RESET) {
       e.status = ALEPH_B200_UNSUPPORTED_INSTRUCTION;
@@ -559,6 +626,7 @@ static int lower_stream(aleph_b200_handle* h, uint32_t n, const aleph_b200_instr
         std::snprintf(e.kind, sizeof(e.kind), "diagonal phase terms");
         return report(h, e);
       }
+      if (relabel && mapped()) settle_relabeling(phys, swaps, (uint32_t)i, ops);  // its masks are logical
       ops.emplace_back();
       if (lower_diagonal_phase(pools->terms + g.data_offset, g.data_len, pools->cond_pool, pools->n_conds, &ops.back(),
                                &e))
@@ -570,6 +638,7 @@ static int lower_stream(aleph_b200_handle* h, uint32_t n, const aleph_b200_instr
       return report(h, e);
     }
   }
+  if (relabel && mapped()) settle_relabeling(phys, swaps, count ? (uint32_t)(count - 1) : 0, ops);
   return ALEPH_B200_OK;
 }
 
@@ -831,6 +900,7 @@ int aleph_b200_apply_diagonal_phase(aleph_b200_handle* h, aleph_b200_state* st, 
   return execute(h, st, P, nullptr, 0, nullptr, nullptr);
 }
 
+// In place, as at most two involution passes (no second state buffer).
 int aleph_b200_unpermute(aleph_b200_handle* h, aleph_b200_state* st, const uint32_t* perm, uint32_t n) {
   if (!h || !st || !perm) return ALEPH_B200_INVALID_ARGUMENT;
   if (n != st->n) return set_error(h, ALEPH_B200_INVALID_ARGUMENT, "perm length %u != num_qubits %u", n, st->n);
@@ -841,23 +911,15 @@ int aleph_b200_unpermute(aleph_b200_handle* h, aleph_b200_state* st, const uint3
     seen |= 1ull << perm[i];
   }
   if (int r = bind(h)) return r;
-  void* tmp = nullptr;
-  CK(cudaMalloc(&tmp, st->bytes), "unpermute buffer");
-  uint32_t* dperm = nullptr;
-  cudaError_t e = cudaMalloc(&dperm, 64 * 4);
-  if (e == cudaSuccess) e = copy_async(h, dperm, perm, n * 4, cudaMemcpyHostToDevice, h->stream);
-  if (e == cudaSuccess) e = launch_unpermute(st->amps, tmp, st->precision, n, dperm, h->stream);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
-  if (e != cudaSuccess) {
-    cudaFree(tmp);
-    cudaFree(dperm);
-    return cuda_fail(h, e, "unpermute");
+  Plan P;
+  for (auto& sigma : split_into_involutions(std::vector<uint32_t>(perm, perm + n))) {
+    Pass ps{};
+    ps.kind = PASS_PERMUTE;
+    for (uint32_t q = 0; q < n; ++q) ps.sigma[q] = sigma[q];
+    P.passes.push_back(ps);
   }
-  cudaFree(st->amps);
-  cudaFree(dperm);
-  st->amps = tmp;
-  h->stats.kernel_launches++;
-  return ALEPH_B200_OK;
+  if (P.passes.empty()) return ALEPH_B200_OK;
+  return execute(h, st, P, nullptr, 0, nullptr, nullptr);
 }
 
 int aleph_b200_measure(aleph_b200_handle* h, aleph_b200_state* st, uint32_t qubit, double u, int* outcome,
@@ -1243,6 +1305,10 @@ int aleph_b200_set_tuning(aleph_b200_handle* h, const char* key, int64_t value) 
     h->opts.smem_max_n = (uint32_t)value;
     return ALEPH_B200_OK;
   }
+  if (!std::strcmp(key, "relabel_swaps")) {
+    h->opts.relabel_swaps = value != 0;
+    return ALEPH_B200_OK;
+  }
   return set_error(h, ALEPH_B200_INVALID_ARGUMENT, "unknown tuning key %s", key);
 }
 
@@ -1260,6 +1326,7 @@ int aleph_b200_describe_plan(uint32_t num_qubits, const aleph_b200_plan_config* 
   tmp.opts.tensor_blocks = config->precision == ALEPH_B200_TC32;
   tmp.opts.block_window_search = config->block_window_search != 0;
   tmp.opts.tile_occupancy = config->tile_occupancy;
+  tmp.opts.relabel_swaps = config->keep_swaps == 0;
   std::vector<Lowered> ops;
   if (int r = lower_stream(&tmp, num_qubits, in, count, pools, &ops)) return r;
   Plan P;

@@ -73,13 +73,26 @@ struct BlockPass {
   uint32_t pre_begin, pre_count, post_begin, post_count;
 };
 
-enum PassKind : uint8_t { PASS_TILE = 1, PASS_SMEM = 2, PASS_KQ = 3, PASS_MEASURE = 4, PASS_BLOCK = 5 };
+// Kind 6 is the renormalisation that follows a tensor-core stream (pass records only).
+enum PassKind : uint8_t {
+  PASS_TILE = 1,
+  PASS_SMEM = 2,
+  PASS_KQ = 3,
+  PASS_MEASURE = 4,
+  PASS_BLOCK = 5,
+  PASS_PERMUTE = 7,
+};
+
+constexpr uint32_t kMaxQubits = 40;
 
 struct Pass {
   PassKind kind;
   TilePass tile;       // PASS_TILE (also op range for PASS_SMEM / PASS_KQ)
   BlockPass block;     // PASS_BLOCK
   uint32_t qubit;      // PASS_MEASURE
+  // PASS_PERMUTE: an involution of the qubit positions; the pass maps
+  // psi(j) -> psi(sigma(j)), sigma(j) moving bit q of j to position sigma[q]
+  uint8_t sigma[kMaxQubits];
   uint32_t record;     // instruction index (errors, outcome slot)
   uint32_t gates;      // gates consumed (stats / cost model)
   // cost-model features: non-diagonal ops on lane qubits, all non-diagonal ops, diagonal ops
@@ -97,6 +110,11 @@ struct Lowered {
   uint32_t record;           // source instruction index
   bool is_measure = false;
   uint32_t measure_qubit = 0;
+  // a qubit-permutation pass (an involution of the positions, see Pass::sigma);
+  // `gates` SWAP records were absorbed into it
+  bool is_permute = false;
+  std::vector<uint8_t> sigma;
+  uint32_t gates = 0;
   // OP_POLY terms (DiagonalPhase): angle, condition count, condition masks
   std::vector<double> poly_angle;
   std::vector<uint32_t> poly_cnt;
@@ -123,6 +141,7 @@ struct PlanOptions {
   uint32_t block_k = 6;
   bool block_window_search = true;  // TC32: also try every 6-qubit window per pass
   uint32_t tile_occupancy = 0;      // tile kernel variant: 128-thread blocks per SM (0 = 2)
+  bool relabel_swaps = true;        // SWAPs relabel qubits; one permutation pass settles the map
 };
 
 // ---------------------------------------------------------------------------
@@ -198,8 +217,14 @@ cudaError_t launch_block_pass(void* amps, const BlockPass& p, const uint8_t* ima
 cudaError_t launch_renormalize(void* amps, int precision, uint32_t n, double* partials, uint32_t nblocks, double* out2,
                                cudaStream_t s);
 cudaError_t launch_convert(const void* src, int src_prec, void* dst, int dst_prec, uint64_t count, cudaStream_t s);
-cudaError_t launch_unpermute(const void* src, void* dst, int precision, uint32_t n, const uint32_t* perm_dev,
-                             cudaStream_t s);
+// In-place qubit-permutation pass: psi(j) -> psi(sigma(j)) for an involution
+// sigma of the n qubit positions (sigma[sigma[q]] == q).
+cudaError_t launch_permute_pass(void* amps, int precision, uint32_t n, const uint8_t* sigma, int sm_count,
+                                cudaStream_t s);
+// Splits the position permutation pi (bit q of an index moves to pi[q]) into
+// involutions applied in order: psi o pi = P_last ... P_first psi, where a
+// pass P_sigma maps psi(j) -> psi(sigma(j)). At most two; none for the identity.
+std::vector<std::vector<uint8_t>> split_into_involutions(const std::vector<uint32_t>& pi);
 
 // readout (kernels_readout.cu)
 // partial sums: out[0] = sum |a|^2, out[1] = count of non-finite |a|^2

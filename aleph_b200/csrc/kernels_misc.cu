@@ -1,6 +1,6 @@
 // kernels_misc.cu — shared-memory whole-state pass (n <= 12), dense k-qubit
-// UnitaryKq pass, state initialisation, precision conversion and the bit
-// permutation of unpermute_state.
+// UnitaryKq pass, state initialisation, precision conversion and the in-place
+// qubit permutation (relabelled SWAPs, unpermute_state).
 //
 // Semantics follow the reference kernels: pair/quartet butterflies
 // (crates/aleph-sv/src/kernels/aos.rs:192-223, :1335-1394), MSB-first operand
@@ -8,6 +8,7 @@
 // mask over the basis index (aos.rs:198-205).
 
 #include <cstdio>
+#include <cstring>
 
 #include "common.cuh"
 
@@ -182,29 +183,146 @@ cudaError_t launch_convert(const void* src, int sp, void* dst, int dp, uint64_t 
   return cudaGetLastError();
 }
 
-// bit_permute_buf (crates/aleph-core/src/perm.rs:25-40): out[i] = in[j],
-// j = sum over logical bits lq of i of (1 << perm[lq]).
+// ---- in-place qubit permutation (an involution sigma of the positions) ------
+// psi(j) -> psi(sigma(j)). Used for relabelled SWAP networks and for
+// unpermute_state (bit_permute_buf, crates/aleph-core/src/perm.rs:25-40, as at
+// most two such passes).
+//
+// Tiles: the tile bits T are the lane qubits 0..4, their images under sigma,
+// and further sigma-closed qubits up to 10 bits; the outer bits O are the
+// rest, also sigma-closed. Outer value h maps to outer value sigma(h), so a
+// CTA takes the pair (h, sigma(h)) at its smaller member, stages both tiles
+// in shared memory and writes each into the other with the tile-local
+// permutation applied. Global reads and writes run along qubits 0..4
+// (32-amplitude runs); shared memory is XOR-swizzled so that reads at the
+// permuted local index stay conflict-free.
+namespace perm {
+
+constexpr int THREADS = 256;
+constexpr int MAX_TILE_BITS = 10;
+constexpr int MAX_TILE = 1 << MAX_TILE_BITS;
+constexpr int PER_THREAD = MAX_TILE / THREADS;
+
+struct Geometry {
+  uint32_t tile_bits;                 // |T|
+  uint32_t n_outer;                   // |O|
+  uint32_t local_identity;            // sigma fixes every tile bit: self-mapped tiles stay put
+  uint8_t ob[kMaxQubits];             // outer positions, ascending
+  uint8_t osig[kMaxQubits];           // index in ob of sigma(ob[m])
+  uint64_t dep_hi[32];                // global offset of local bits 5.. (indexed by local >> 5)
+  uint16_t sig_lo[32], sig_hi[32];    // local sigma: sig_lo[local & 31] ^ sig_hi[local >> 5]
+};
+
+__device__ __forceinline__ uint32_t swz(uint32_t o) { return o ^ ((o >> 5) & 31u); }
+
 template <typename Real>
-__global__ void unpermute_kernel(const V2<Real>* __restrict__ src, V2<Real>* __restrict__ dst, uint32_t n,
-                                 const uint32_t* __restrict__ perm) {
-  const uint64_t len = 1ull << n;
-  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < len; i += (uint64_t)gridDim.x * blockDim.x) {
-    uint64_t j = 0;
-    for (uint32_t lq = 0; lq < n; ++lq)
-      if ((i >> lq) & 1) j |= 1ull << __ldg(&perm[lq]);
-    dst[i] = ld_amp<Real>(src + j);
+__global__ void __launch_bounds__(THREADS) permute_kernel(V2<Real>* __restrict__ X, const Geometry g) {
+  __shared__ V2<Real> S1[MAX_TILE], S2[MAX_TILE];
+  const uint32_t T = 1u << g.tile_bits;
+  const uint64_t nh = 1ull << g.n_outer;
+  for (uint64_t h = blockIdx.x; h < nh; h += gridDim.x) {
+    uint64_t h2 = 0, b1 = 0, b2 = 0;
+    for (uint32_t m = 0; m < g.n_outer; ++m) {
+      const uint64_t bit = (h >> m) & 1ull;
+      h2 |= bit << g.osig[m];
+      b1 |= bit << g.ob[m];
+      b2 |= bit << g.ob[g.osig[m]];
+    }
+    if (h2 < h) continue;  // the pair belongs to its smaller member (uniform across the CTA)
+    const bool pair = h2 != h;
+    if (!pair && g.local_identity) continue;  // a fixed tile: nothing moves
+    V2<Real> r1[PER_THREAD], r2[PER_THREAD];
+#pragma unroll
+    for (int k = 0; k < PER_THREAD; ++k) {
+      const uint32_t o = threadIdx.x + (uint32_t)k * THREADS;
+      if (o < T) {
+        const uint64_t off = (o & 31u) | g.dep_hi[o >> 5];
+        r1[k] = X[b1 + off];
+        if (pair) r2[k] = X[b2 + off];
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < PER_THREAD; ++k) {
+      const uint32_t o = threadIdx.x + (uint32_t)k * THREADS;
+      if (o < T) {
+        S1[swz(o)] = r1[k];
+        if (pair) S2[swz(o)] = r2[k];
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < PER_THREAD; ++k) {
+      const uint32_t o = threadIdx.x + (uint32_t)k * THREADS;
+      if (o < T) {
+        const uint32_t s = swz((uint32_t)g.sig_lo[o & 31u] ^ (uint32_t)g.sig_hi[o >> 5]);
+        const uint64_t off = (o & 31u) | g.dep_hi[o >> 5];
+        X[b1 + off] = pair ? S2[s] : S1[s];
+        if (pair) X[b2 + off] = S1[s];
+      }
+    }
+    __syncthreads();
   }
 }
 
-cudaError_t launch_unpermute(const void* src, void* dst, int precision, uint32_t n, const uint32_t* perm_dev,
-                             cudaStream_t s) {
-  const uint64_t len = 1ull << n;
-  const uint64_t b = (len + 255) / 256;
-  const unsigned blocks = (unsigned)(b > 148ull * 32 ? 148ull * 32 : b);
+// Tile geometry of an involution (host side).
+static Geometry geometry(uint32_t n, const uint8_t* sigma) {
+  Geometry g;
+  std::memset(&g, 0, sizeof(g));
+  const uint32_t nl = n < 5 ? n : 5;
+  const uint32_t want = n < (uint32_t)MAX_TILE_BITS ? n : (uint32_t)MAX_TILE_BITS;
+  uint64_t T = 0;
+  for (uint32_t q = 0; q < nl; ++q) T |= (1ull << q) | (1ull << sigma[q]);
+  auto count = [&]() { return (uint32_t)__builtin_popcountll(T); };
+  for (uint32_t q = 0; q < n && count() < want; ++q)  // fixed points first
+    if (!((T >> q) & 1) && sigma[q] == q) T |= 1ull << q;
+  for (uint32_t q = 0; q < n && count() + 2 <= want; ++q)  // then transposed pairs
+    if (!((T >> q) & 1)) T |= (1ull << q) | (1ull << sigma[q]);
+  uint8_t tb[kMaxQubits], local_of[kMaxQubits], outer_of[kMaxQubits];
+  uint32_t k = 0, m = 0;
+  for (uint32_t q = 0; q < n; ++q) {
+    if ((T >> q) & 1) {
+      local_of[q] = (uint8_t)k;
+      tb[k++] = (uint8_t)q;
+    } else {
+      outer_of[q] = (uint8_t)m;
+      g.ob[m++] = (uint8_t)q;
+    }
+  }
+  g.tile_bits = k;
+  g.n_outer = m;
+  g.local_identity = 1;
+  for (uint32_t j = 0; j < k; ++j) g.local_identity &= sigma[tb[j]] == tb[j] ? 1u : 0u;
+  for (uint32_t j = 0; j < m; ++j) g.osig[j] = outer_of[sigma[g.ob[j]]];
+  for (uint32_t x = 0; x < 32; ++x) {
+    uint32_t lo = 0, hi = 0;
+    uint64_t dep = 0;
+    for (uint32_t b = 0; b < 5; ++b) {
+      if (!((x >> b) & 1)) continue;
+      if (b < k) lo |= 1u << local_of[sigma[tb[b]]];
+      if (5 + b < k) {
+        hi |= 1u << local_of[sigma[tb[5 + b]]];
+        dep |= 1ull << tb[5 + b];
+      }
+    }
+    g.sig_lo[x] = (uint16_t)lo;
+    g.sig_hi[x] = (uint16_t)hi;
+    g.dep_hi[x] = dep;
+  }
+  return g;
+}
+
+}  // namespace perm
+
+cudaError_t launch_permute_pass(void* amps, int precision, uint32_t n, const uint8_t* sigma, int sm_count,
+                                cudaStream_t s) {
+  const perm::Geometry g = perm::geometry(n, sigma);
+  const uint64_t nh = 1ull << g.n_outer;
+  const uint64_t want = (uint64_t)(sm_count > 0 ? sm_count : 148) * 6;
+  const unsigned blocks = (unsigned)(nh < want ? nh : want);
   if (precision == ALEPH_B200_F64)
-    unpermute_kernel<double><<<blocks, 256, 0, s>>>((const double2*)src, (double2*)dst, n, perm_dev);
+    perm::permute_kernel<double><<<blocks, perm::THREADS, 0, s>>>((double2*)amps, g);
   else
-    unpermute_kernel<float><<<blocks, 256, 0, s>>>((const float2*)src, (float2*)dst, n, perm_dev);
+    perm::permute_kernel<float><<<blocks, perm::THREADS, 0, s>>>((float2*)amps, g);
   return cudaGetLastError();
 }
 

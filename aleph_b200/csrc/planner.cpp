@@ -845,6 +845,35 @@ int plan_segment_blocks(const std::vector<const Lowered*>& seg, uint32_t n, uint
 
 }  // namespace
 
+// A cycle c_0 -> c_1 -> ... -> c_{m-1} -> c_0 of pi is alpha o beta with the
+// reflections beta(c_i) = c_{-i} and alpha(c_i) = c_{1-i} (indices mod m), both
+// involutions; alpha is applied first (P_beta P_alpha psi = psi o alpha o beta).
+std::vector<std::vector<uint8_t>> split_into_involutions(const std::vector<uint32_t>& pi) {
+  const uint32_t n = (uint32_t)pi.size();
+  std::vector<uint8_t> alpha(n), beta(n);
+  std::vector<bool> seen(n, false);
+  bool alpha_id = true, beta_id = true;
+  for (uint32_t s = 0; s < n; ++s) {
+    if (seen[s]) continue;
+    std::vector<uint32_t> cyc;
+    for (uint32_t q = s; !seen[q]; q = pi[q]) {
+      seen[q] = true;
+      cyc.push_back(q);
+    }
+    const uint32_t m = (uint32_t)cyc.size();
+    for (uint32_t i = 0; i < m; ++i) {
+      beta[cyc[i]] = (uint8_t)cyc[(m - i) % m];
+      alpha[cyc[i]] = (uint8_t)cyc[(m + 1 - i) % m];
+      beta_id &= beta[cyc[i]] == cyc[i];
+      alpha_id &= alpha[cyc[i]] == cyc[i];
+    }
+  }
+  std::vector<std::vector<uint8_t>> out;
+  if (!alpha_id) out.push_back(alpha);
+  if (!beta_id) out.push_back(beta);
+  return out;
+}
+
 int build_plan(const std::vector<Lowered>& ops, uint32_t n, const PlanOptions& o, Plan* P) {
   std::vector<const Lowered*> seg;
   int status = ALEPH_B200_OK;
@@ -878,6 +907,14 @@ int build_plan(const std::vector<Lowered>& ops, uint32_t n, const PlanOptions& o
       ps.record = L.record;
       P->passes.push_back(ps);
       ++P->n_measures;
+    } else if (L.is_permute) {
+      flush();
+      Pass ps{};
+      ps.kind = PASS_PERMUTE;
+      for (uint32_t q = 0; q < n && q < kMaxQubits; ++q) ps.sigma[q] = L.sigma[q];
+      ps.record = L.record;
+      ps.gates = L.gates;
+      P->passes.push_back(ps);
     } else {
       seg.push_back(&L);
     }

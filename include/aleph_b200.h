@@ -244,7 +244,8 @@ int aleph_b200_qaoa_sweep(aleph_b200_handle* h, uint32_t p, const aleph_b200_qao
 int aleph_b200_apply_diagonal_phase(aleph_b200_handle* h, aleph_b200_state* st, const aleph_b200_phase_term* terms,
                                     uint64_t n_terms, const uint64_t* cond_pool, uint64_t n_conds);
 
-/* ---- Backend::unpermute_state (crates/aleph-core/src/perm.rs:25-40): perm[logical] = physical ---- */
+/* ---- Backend::unpermute_state (crates/aleph-core/src/perm.rs:25-40): perm[logical] = physical ----
+ * In place: at most two involution passes, no second state buffer. */
 int aleph_b200_unpermute(aleph_b200_handle* h, aleph_b200_state* st, const uint32_t* perm, uint32_t n);
 
 /* ---- Backend::measure (crates/aleph-sv/src/measure.rs:41-102) ----
@@ -305,13 +306,17 @@ int aleph_b200_last_error_info(const aleph_b200_handle* h, aleph_b200_error_info
 /* ---- planner tuning (the autotuner's knobs) ----
  * keys: "tile_r" (register qubits per warp tile, 1..5), "smem_max_n" (states
  * with n <= this run as one shared-memory pass, 0..12), "record_passes"
- * (0/1: time every pass of later gate streams with CUDA events). */
+ * (0/1: time every pass of later gate streams with CUDA events),
+ * "relabel_swaps" (0/1, default 1: an uncontrolled SWAP of a state larger
+ * than smem_max_n relabels qubits instead of moving data, and one or two
+ * in-place permutation passes settle the labels at the end of the stream). */
 int aleph_b200_set_tuning(aleph_b200_handle* h, const char* key, int64_t value);
 
 /* ---- per-pass timing records (training data of the learned fusion planner) ---- */
 typedef struct aleph_b200_pass_record {
   uint32_t kind;        /* 1 = CUDA-core tile pass, 2 = shared-memory pass, 3 = dense k-qubit,
-                           4 = measurement, 5 = tensor-core dense block, 6 = renormalisation */
+                           4 = measurement, 5 = tensor-core dense block, 6 = renormalisation,
+                           7 = qubit permutation (relabelled SWAPs, unpermute)             */
   uint32_t gates;       /* gates the pass applied                                          */
   uint32_t n;           /* state qubits                                                    */
   uint32_t nq;          /* entries used in qubits[]                                        */
@@ -336,6 +341,7 @@ typedef struct aleph_b200_plan_config {
   uint32_t smem_max_n;           /* n <= this: one shared-memory pass        */
   uint32_t block_window_search;  /* TC32: also try every 6-qubit window      */
   uint32_t tile_occupancy;       /* tile kernel variant: 0 (default) or 2..4 */
+  uint32_t keep_swaps;           /* 1: SWAP records run as gates; 0: relabel */
 } aleph_b200_plan_config;
 int aleph_b200_describe_plan(uint32_t num_qubits, const aleph_b200_plan_config* config, const aleph_b200_instr* instrs,
                              uint64_t count, const aleph_b200_pools* pools, aleph_b200_pass_record* out, uint64_t cap,

@@ -196,6 +196,35 @@ def test_describe_plan_reports_validation_errors():
     assert e.value.status == abi.QUBIT_OUT_OF_RANGE
 
 
+def test_swaps_relabel_into_permutation_passes():
+    from aleph_b200.backend import BackendError, describe_plan
+
+    def kinds(n, instrs, **kw):
+        return [p["kind"] for p in describe_plan(n, instrs, **kw)]
+
+    sw = lambda a, b, ctrl=(): C.GateInstance(C.Gate("Swap"), [a, b], list(ctrl))
+    # the QFT's bit reversal is one involution: one permutation pass instead of tile passes
+    c = workloads.qft_product(30, 0)
+    on, off = describe_plan(30, c.instructions), describe_plan(30, c.instructions, relabel_swaps=False)
+    assert [p["kind"] for p in on].count("permute") == 1 and "permute" not in [p["kind"] for p in off]
+    assert len(on) <= len(off) - 4
+    assert sum(p["gates"] for p in on) == sum(p["gates"] for p in off) == c.gate_count()
+    # a 3-cycle of qubit labels is two involutions; a swap undone costs nothing
+    assert kinds(20, [sw(0, 1), sw(1, 2)]) == ["permute", "permute"]
+    assert kinds(20, [sw(3, 17), sw(17, 3)]) == []
+    assert kinds(20, [sw(3, 17)]) == ["permute"]
+    # a controlled SWAP is a gate; so is any SWAP of a state that fits one shared-memory pass
+    assert kinds(20, [sw(3, 17, [5])]) == ["tile"]
+    assert kinds(12, [sw(3, 7)]) == ["smem"]
+    # the labels settle before a DiagonalPhase record, whose masks are logical
+    dp = C.DiagonalPhase(20, [C.PhaseTerm((1 << 19,), 0.5)])
+    assert kinds(20, [sw(0, 19), dp, C.GateInstance(C.H(), [0])]) == ["permute", "tile"]
+    # errors name the qubits as written, and a bad SWAP is still rejected
+    with pytest.raises(BackendError) as e:
+        describe_plan(20, [sw(0, 19), sw(4, 20)])
+    assert e.value.status == abi.QUBIT_OUT_OF_RANGE
+
+
 # ---- learned planner: host logic ---------------------------------------------------------
 def test_learned_candidates_and_features():
     from aleph_b200 import learned
