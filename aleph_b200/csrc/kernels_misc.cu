@@ -215,52 +215,95 @@ struct Geometry {
 
 __device__ __forceinline__ uint32_t swz(uint32_t o) { return o ^ ((o >> 5) & 31u); }
 
+// The CTA's work items: outer values h (grid-stride) that own a pair or a
+// self-mapped tile that moves. Uniform across the CTA.
+struct Item {
+  uint64_t h, b1, b2;
+  bool pair;
+};
+
+// This lane's outer bit m = lane (n_outer <= 31): its positions under h, in
+// sigma(h) (compact) and in the partner tile's base offset.
+struct LaneBit {
+  bool act;
+  uint32_t m, to_h2, to_b1, to_b2;
+};
+
+__device__ __forceinline__ uint64_t or_across_warp(uint64_t x) {
+  const uint32_t lo = __reduce_or_sync(0xffffffffu, (uint32_t)x);
+  const uint32_t hi = __reduce_or_sync(0xffffffffu, (uint32_t)(x >> 32));
+  return (uint64_t)hi << 32 | lo;
+}
+
+// Every warp decodes h with one lane per outer bit (no per-thread bit loop).
+__device__ __forceinline__ Item next_item(const Geometry& g, const LaneBit& lb, uint64_t h, uint64_t nh) {
+  for (; h < nh; h += gridDim.x) {
+    const uint64_t bit = lb.act ? (h >> lb.m) & 1ull : 0ull;
+    const uint64_t h2 = or_across_warp(bit << lb.to_h2);
+    if (h2 < h) continue;                     // the pair belongs to its smaller member
+    if (h2 == h && g.local_identity) continue;  // a fixed tile: nothing moves
+    return Item{h, or_across_warp(bit << lb.to_b1), or_across_warp(bit << lb.to_b2), h2 != h};
+  }
+  return Item{nh, 0, 0, false};
+}
+
+// Software pipeline: the next item's loads are issued once the current item
+// sits in shared memory, and are in flight during its write-back.
 template <typename Real>
 __global__ void __launch_bounds__(THREADS) permute_kernel(V2<Real>* __restrict__ X, const Geometry g) {
   __shared__ V2<Real> S1[MAX_TILE], S2[MAX_TILE];
   const uint32_t T = 1u << g.tile_bits;
   const uint64_t nh = 1ull << g.n_outer;
-  for (uint64_t h = blockIdx.x; h < nh; h += gridDim.x) {
-    uint64_t h2 = 0, b1 = 0, b2 = 0;
-    for (uint32_t m = 0; m < g.n_outer; ++m) {
-      const uint64_t bit = (h >> m) & 1ull;
-      h2 |= bit << g.osig[m];
-      b1 |= bit << g.ob[m];
-      b2 |= bit << g.ob[g.osig[m]];
-    }
-    if (h2 < h) continue;  // the pair belongs to its smaller member (uniform across the CTA)
-    const bool pair = h2 != h;
-    if (!pair && g.local_identity) continue;  // a fixed tile: nothing moves
-    V2<Real> r1[PER_THREAD], r2[PER_THREAD];
+  // lane-indexed parameters are read once (a lane-divergent read of the
+  // parameter bank serialises across the warp)
+  const uint32_t lane = threadIdx.x & 31u;
+  LaneBit lb;
+  lb.m = lane;
+  lb.act = lane < g.n_outer;
+  lb.to_h2 = lb.act ? g.osig[lane] : 0u;
+  lb.to_b1 = lb.act ? g.ob[lane] : 0u;
+  lb.to_b2 = lb.act ? g.ob[g.osig[lane]] : 0u;
+  const uint32_t sig_lane = g.sig_lo[lane];  // local bits 0..4 of o are the lane
+  V2<Real> r1[PER_THREAD], r2[PER_THREAD];
+  auto load = [&](const Item& it) {
 #pragma unroll
     for (int k = 0; k < PER_THREAD; ++k) {
       const uint32_t o = threadIdx.x + (uint32_t)k * THREADS;
       if (o < T) {
         const uint64_t off = (o & 31u) | g.dep_hi[o >> 5];
-        r1[k] = X[b1 + off];
-        if (pair) r2[k] = X[b2 + off];
+        r1[k] = X[it.b1 + off];
+        if (it.pair) r2[k] = X[it.b2 + off];
       }
     }
+  };
+  Item cur = next_item(g, lb, blockIdx.x, nh);
+  if (cur.h >= nh) return;
+  load(cur);
+  for (;;) {
+    __syncthreads();  // the previous write-back is done reading shared memory
 #pragma unroll
     for (int k = 0; k < PER_THREAD; ++k) {
       const uint32_t o = threadIdx.x + (uint32_t)k * THREADS;
       if (o < T) {
         S1[swz(o)] = r1[k];
-        if (pair) S2[swz(o)] = r2[k];
+        if (cur.pair) S2[swz(o)] = r2[k];
       }
     }
     __syncthreads();
+    const Item nxt = next_item(g, lb, cur.h + gridDim.x, nh);
+    if (nxt.h < nh) load(nxt);
 #pragma unroll
     for (int k = 0; k < PER_THREAD; ++k) {
       const uint32_t o = threadIdx.x + (uint32_t)k * THREADS;
       if (o < T) {
-        const uint32_t s = swz((uint32_t)g.sig_lo[o & 31u] ^ (uint32_t)g.sig_hi[o >> 5]);
+        const uint32_t s = swz(sig_lane ^ (uint32_t)g.sig_hi[o >> 5]);
         const uint64_t off = (o & 31u) | g.dep_hi[o >> 5];
-        X[b1 + off] = pair ? S2[s] : S1[s];
-        if (pair) X[b2 + off] = S1[s];
+        X[cur.b1 + off] = cur.pair ? S2[s] : S1[s];
+        if (cur.pair) X[cur.b2 + off] = S1[s];
       }
     }
-    __syncthreads();
+    if (nxt.h >= nh) break;
+    cur = nxt;
   }
 }
 
@@ -316,10 +359,22 @@ static Geometry geometry(uint32_t n, const uint8_t* sigma) {
 cudaError_t launch_permute_pass(void* amps, int precision, uint32_t n, const uint8_t* sigma, int sm_count,
                                 cudaStream_t s) {
   const perm::Geometry g = perm::geometry(n, sigma);
+  if (g.n_outer > 31) return cudaErrorInvalidValue;  // one lane per outer bit
   const uint64_t nh = 1ull << g.n_outer;
-  const uint64_t want = (uint64_t)(sm_count > 0 ? sm_count : 148) * 6;
+  // a persistent grid: exactly the CTAs that are resident at once
+  static int resident[2] = {0, 0};
+  const int k = precision == ALEPH_B200_F64 ? 1 : 0;
+  if (!resident[k]) {
+    int nb = 0;
+    const cudaError_t e =
+        k ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, perm::permute_kernel<double>, perm::THREADS, 0)
+          : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, perm::permute_kernel<float>, perm::THREADS, 0);
+    if (e != cudaSuccess) return e;
+    resident[k] = nb > 0 ? nb : 1;
+  }
+  const uint64_t want = (uint64_t)(sm_count > 0 ? sm_count : 148) * (uint64_t)resident[k];
   const unsigned blocks = (unsigned)(nh < want ? nh : want);
-  if (precision == ALEPH_B200_F64)
+  if (k)
     perm::permute_kernel<double><<<blocks, perm::THREADS, 0, s>>>((double2*)amps, g);
   else
     perm::permute_kernel<float><<<blocks, perm::THREADS, 0, s>>>((float2*)amps, g);
