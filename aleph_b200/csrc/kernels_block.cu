@@ -45,6 +45,7 @@
 #include <cstdint>
 #include <cstring>
 
+#include <cuda.h>  // CUtensorMap and its enums (the encoder is fetched through the runtime)
 #include <cuda_bf16.h>
 
 #include "common.cuh"
@@ -117,6 +118,42 @@ __device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_
       "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
       "l"(src), "r"(bytes), "r"(bar)
       : "memory");
+}
+// One tiled tensor copy (no multicast) of the box at coordinates c[0..rank)
+// into shared memory, completing `bar`'s transaction count.
+__device__ __forceinline__ void tensor_load(uint32_t dst, const CUtensorMap* map, uint32_t rank, const int32_t* c,
+                                            uint32_t bar) {
+  const uint64_t m = reinterpret_cast<uint64_t>(map);
+  switch (rank) {
+    case 2:
+      asm volatile(
+          "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+              dst),
+          "l"(m), "r"(c[0]), "r"(c[1]), "r"(bar)
+          : "memory");
+      break;
+    case 3:
+      asm volatile(
+          "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+          "[%5];" ::"r"(dst),
+          "l"(m), "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(bar)
+          : "memory");
+      break;
+    case 4:
+      asm volatile(
+          "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+          "[%6];" ::"r"(dst),
+          "l"(m), "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(c[3]), "r"(bar)
+          : "memory");
+      break;
+    default:
+      asm volatile(
+          "cp.async.bulk.tensor.5d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5, "
+          "%6}], [%7];" ::"r"(dst),
+          "l"(m), "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(c[3]), "r"(c[4]), "r"(bar)
+          : "memory");
+      break;
+  }
 }
 __device__ __forceinline__ void fence_barrier_init() {
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -201,8 +238,19 @@ __host__ __device__ __forceinline__ uint32_t sw128_off(uint32_t r, uint32_t k, u
   return region * rows * 128 + (r >> 3) * 1024 + (r & 7) * 128 + ((((kk >> 3) ^ (r & 7)) & 7) << 4) + ((kk & 7) << 1);
 }
 
-__device__ __forceinline__ uint32_t bf16_bits(float x) { return (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(x)); }
-__device__ __forceinline__ float bf16_val(uint32_t b) { return __uint_as_float(b << 16); }
+// Two floats to BF16 (round to nearest even) in one instruction: lo -> bits
+// 0..15, hi -> bits 16..31.
+__device__ __forceinline__ uint32_t bf16x2_bits(float lo, float hi) {
+  uint32_t d;
+  asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(hi), "f"(lo));
+  return d;
+}
+// Split a pair of floats into packed BF16 hi and lo parts, x = hi + lo to ~16 bits.
+__device__ __forceinline__ void split_pair(float x0, float x1, uint32_t& hi, uint32_t& lo) {
+  hi = bf16x2_bits(x0, x1);
+  const float h0 = __uint_as_float(hi << 16), h1 = __uint_as_float(hi & 0xffff0000u);
+  lo = bf16x2_bits(x0 - h0, x1 - h1);
+}
 
 }  // namespace blk
 
@@ -212,6 +260,15 @@ struct BlockArgs {
   const uint8_t* image;   // W_hi | W_lo, 64 KiB, swizzled
   const Op* post;         // diagonal ops applied after the block
   uint32_t post_count;
+  // Tensor-map load of a whole tile (blocks with no qubit below 7): the state
+  // as an FP32 tensor whose dim 0 is qubits 0..6 (256 floats) and whose
+  // other dims are the maximal groups of consecutive block / non-block
+  // qubits above; the box is the tile (block groups at full extent). The
+  // coordinate of a non-block group is the tile index bits (t >> tshift) &
+  // tmaskc.
+  CUtensorMap tmap;
+  uint32_t trank;  // 0: per-run bulk copies instead
+  uint32_t tshift[5], tmaskc[5];
   const float2* coef;
   PolyTables poly;
   int* err;
@@ -333,10 +390,22 @@ __global__ void __launch_bounds__(blk::THREADS, 1) block_kernel(const __grid_con
         abort_sh = 1;
         break;
       }
+      const uint32_t dst0 = sbase + OFF_S + s * STAGE_BYTES;
+      if (a.trank) {
+        // the whole tile as one tensor box: the copy engine's cost is per
+        // copy (~100 cycles), so one box beats 64 runs of 1 KiB
+        if (lane == 0) {
+          mbar_expect_tx(bar_sfull + 8 * s, TILE_BYTES);
+          int32_t crd[5];
+#pragma unroll
+          for (int d = 0; d < 5; ++d) crd[d] = (int32_t)((t >> a.tshift[d]) & a.tmaskc[d]);
+          tensor_load(dst0, &a.tmap, a.trank, crd, bar_sfull + 8 * s);
+        }
+        continue;
+      }
       const uint64_t base = tile_base(t);
       if (lane == 0) mbar_expect_tx(bar_sfull + 8 * s, TILE_BYTES);
       __syncwarp();
-      const uint32_t dst0 = sbase + OFF_S + s * STAGE_BYTES;
       for (uint32_t r = lane; r < nruns; r += 32)
         bulk_load(dst0 + r * run_stride, a.amps + (base | runoff[r]), run_bytes, bar_sfull + 8 * s);
     }
@@ -364,12 +433,8 @@ __global__ void __launch_bounds__(blk::THREADS, 1) block_kernel(const __grid_con
           const uint32_t r1 = h ? a.rowoff[33 + 2 * p] : a.rowoff[2 * p + 1];
           const float2 x0 = *(const float2*)(stg + r0);
           const float2 x1 = *(const float2*)(stg + r1);
-          const uint32_t a0 = bf16_bits(x0.x), a1 = bf16_bits(x1.x);
-          const uint32_t b0 = bf16_bits(x0.y), b1 = bf16_bits(x1.y);
-          hr[p] = a0 | (a1 << 16);
-          hi[p] = b0 | (b1 << 16);
-          lr[p] = bf16_bits(x0.x - bf16_val(a0)) | (bf16_bits(x1.x - bf16_val(a1)) << 16);
-          li[p] = bf16_bits(x0.y - bf16_val(b0)) | (bf16_bits(x1.y - bf16_val(b1)) << 16);
+          split_pair(x0.x, x1.x, hr[p], lr[p]);
+          split_pair(x0.y, x1.y, hi[p], li[p]);
         }
         // A row layout: K = [Re x_0..63 | Im x_0..63], two BF16 per 32-bit column
         tmem_st16(ta + 16 * h, hr);            // hi, Re part
@@ -604,6 +669,58 @@ void set_tile_geometry(uint32_t n, const uint32_t* bq, BlockArgs* a) {
   }
 }
 
+// The tensor map of a tile box (BlockArgs::tmap) for a block with no qubit
+// below 7 whose tile is 64 unpadded runs of 1 KiB. Leaves trank = 0 (per-run
+// bulk copies) for any other geometry, for more than 5 dimensions, or when
+// the driver's encoder is unavailable or refuses the map.
+void set_tensor_map(uint32_t n, void* amps, BlockArgs* a) {
+  using namespace blk;
+  a->trank = 0;
+  uint64_t bmask = 0;
+  for (int j = 0; j < 6; ++j) bmask |= 1ull << a->bq[j];
+  if ((bmask & 0x7F) || a->nruns != 64 || a->run_bytes != 1024 || a->run_stride != 1024) return;
+  typedef CUresult (*EncodeFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                               const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                               CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+  static EncodeFn encode = nullptr;
+  static bool looked_up = false;
+  if (!looked_up) {
+    looked_up = true;
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      encode = (EncodeFn)fn;
+  }
+  if (!encode) return;
+  cuuint64_t gdim[5], gstride[4];
+  cuuint32_t box[5], estr[5] = {1, 1, 1, 1, 1};
+  gdim[0] = 256;  // qubits 0..6: 128 complex = 256 floats, 1 KiB
+  box[0] = 256;
+  a->tshift[0] = a->tmaskc[0] = 0;
+  uint32_t rank = 1, tbit = 0;
+  for (uint32_t q = 7; q < n;) {
+    const bool blockq = (bmask >> q) & 1;
+    uint32_t len = 0;
+    while (q + len < n && (((bmask >> (q + len)) & 1) != 0) == blockq) ++len;
+    if (rank == 5) return;
+    gdim[rank] = 1ull << len;
+    gstride[rank - 1] = 8ull << q;
+    box[rank] = blockq ? (1u << len) : 1u;
+    a->tshift[rank] = blockq ? 0 : tbit;
+    a->tmaskc[rank] = blockq ? 0 : (uint32_t)((1ull << len) - 1);
+    if (!blockq) tbit += len;
+    ++rank;
+    q += len;
+  }
+  for (uint32_t d = rank; d < 5; ++d) a->tshift[d] = a->tmaskc[d] = 0;
+  if (rank < 2) return;
+  const CUresult r = encode(&a->tmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, rank, amps, gdim, gstride, box, estr,
+                            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r == CUDA_SUCCESS) a->trank = rank;
+}
+
 }  // namespace
 
 cudaError_t launch_block_pass(void* amps, const BlockPass& p, const uint8_t* images, const Op* ops, const void* coef,
@@ -620,6 +737,7 @@ cudaError_t launch_block_pass(void* amps, const BlockPass& p, const uint8_t* ima
   a.n = p.n;
   for (int j = 0; j < 6; ++j) a.bq[j] = p.bq[j];
   set_tile_geometry(p.n, p.bq, &a);
+  set_tensor_map(p.n, amps, &a);
   static uint64_t attr_devices = 0;  // devices on which the shared-memory opt-in is done
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
