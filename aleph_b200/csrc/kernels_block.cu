@@ -268,7 +268,8 @@ struct BlockArgs {
   // tmaskc.
   CUtensorMap tmap;
   uint32_t trank;  // 0: per-run bulk copies instead
-  uint32_t tshift[5], tmaskc[5];
+  uint32_t tbytes;  // bytes one box delivers (the barrier's transaction count)
+  uint32_t tshift[5], tmaskc[5], tmul[5];  // coordinate d = ((t >> tshift) & tmaskc) * tmul
   const float2* coef;
   PolyTables poly;
   int* err;
@@ -395,10 +396,10 @@ __global__ void __launch_bounds__(blk::THREADS, 1) block_kernel(const __grid_con
         // the whole tile as one tensor box: the copy engine's cost is per
         // copy (~100 cycles), so one box beats 64 runs of 1 KiB
         if (lane == 0) {
-          mbar_expect_tx(bar_sfull + 8 * s, TILE_BYTES);
+          mbar_expect_tx(bar_sfull + 8 * s, a.tbytes);
           int32_t crd[5];
 #pragma unroll
-          for (int d = 0; d < 5; ++d) crd[d] = (int32_t)((t >> a.tshift[d]) & a.tmaskc[d]);
+          for (int d = 0; d < 5; ++d) crd[d] = (int32_t)(((t >> a.tshift[d]) & a.tmaskc[d]) * a.tmul[d]);
           tensor_load(dst0, &a.tmap, a.trank, crd, bar_sfull + 8 * s);
         }
         continue;
@@ -414,6 +415,10 @@ __global__ void __launch_bounds__(blk::THREADS, 1) block_kernel(const __grid_con
     const int q = warp & 3;  // TMEM lane quarter
     const int col = 32 * q + lane;
     const uint32_t lc = Lcol[col];
+    // With qubit 0 in the block, block rows 2p and 2p+1 sit 8 bytes apart in
+    // the stage and every row pair starts on a 16-byte boundary (all other
+    // stage strides are multiples of 16).
+    const bool row_pairs = a.bq[0] == 0;
     uint32_t i = 0;
     for (uint64_t t = first; t < ntiles; t += stride, ++i) {
       const uint32_t s = i & 1, ph = (i >> 1) & 1;
@@ -431,8 +436,15 @@ __global__ void __launch_bounds__(blk::THREADS, 1) block_kernel(const __grid_con
         for (int p = 0; p < 16; ++p) {
           const uint32_t r0 = h ? a.rowoff[32 + 2 * p] : a.rowoff[2 * p];
           const uint32_t r1 = h ? a.rowoff[33 + 2 * p] : a.rowoff[2 * p + 1];
-          const float2 x0 = *(const float2*)(stg + r0);
-          const float2 x1 = *(const float2*)(stg + r1);
+          float2 x0, x1;
+          if (row_pairs) {  // rows 2p, 2p+1 adjacent: one 16-byte load
+            const float4 v = *(const float4*)(stg + r0);
+            x0 = make_float2(v.x, v.y);
+            x1 = make_float2(v.z, v.w);
+          } else {
+            x0 = *(const float2*)(stg + r0);
+            x1 = *(const float2*)(stg + r1);
+          }
           split_pair(x0.x, x1.x, hr[p], lr[p]);
           split_pair(x0.y, x1.y, hi[p], li[p]);
         }
@@ -669,16 +681,28 @@ void set_tile_geometry(uint32_t n, const uint32_t* bq, BlockArgs* a) {
   }
 }
 
-// The tensor map of a tile box (BlockArgs::tmap) for a block with no qubit
-// below 7 whose tile is 64 unpadded runs of 1 KiB. Leaves trank = 0 (per-run
-// bulk copies) for any other geometry, for more than 5 dimensions, or when
-// the driver's encoder is unavailable or refuses the map.
+// The tensor map of a tile box (BlockArgs::tmap), for two geometries:
+//  * a block with no qubit below 7, whose tile is 64 unpadded runs of 1 KiB:
+//    dim 0 is qubits 0..6 (256 floats, the box's full width), then the
+//    maximal groups of consecutive block / non-block qubits;
+//  * the block on qubits 0..5 with its columns on qubits 7..13 (above the
+//    gap at qubit 6), whose tile is 128 runs of 512 B each followed by a
+//    16-byte pad: dim 0 is qubits 0..6 and the box takes 132 floats of it
+//    (a column's 64 amplitudes plus 16 bytes that land in the pad; the
+//    tile's qubit-6 bit is the x offset 0 or 128 floats), dim 1 the 128
+//    columns, dim 2 the qubits from 14 up.
+// Leaves trank = 0 (per-run bulk copies) for any other geometry, for more
+// than 5 dimensions, or when the driver's encoder is unavailable or refuses
+// the map.
 void set_tensor_map(uint32_t n, void* amps, BlockArgs* a) {
   using namespace blk;
   a->trank = 0;
   uint64_t bmask = 0;
   for (int j = 0; j < 6; ++j) bmask |= 1ull << a->bq[j];
-  if ((bmask & 0x7F) || a->nruns != 64 || a->run_bytes != 1024 || a->run_stride != 1024) return;
+  const bool high = !(bmask & 0x7F) && a->nruns == 64 && a->run_bytes == 1024 && a->run_stride == 1024;
+  const bool low = bmask == 0x3F && a->tmask == 0x3FBFull && a->nruns == 128 && a->run_bytes == 512 &&
+                   a->run_stride == 528 && n >= 14;
+  if (!high && !low) return;
   typedef CUresult (*EncodeFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                                CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
@@ -695,9 +719,33 @@ void set_tensor_map(uint32_t n, void* amps, BlockArgs* a) {
   if (!encode) return;
   cuuint64_t gdim[5], gstride[4];
   cuuint32_t box[5], estr[5] = {1, 1, 1, 1, 1};
+  for (int d = 0; d < 5; ++d) {
+    a->tshift[d] = a->tmaskc[d] = 0;
+    a->tmul[d] = 1;
+  }
   gdim[0] = 256;  // qubits 0..6: 128 complex = 256 floats, 1 KiB
+  if (low) {
+    box[0] = 132;  // 512 B of a column + 16 B into the pad
+    a->tmaskc[0] = 1;  // tile bit 0 is qubit 6: x = 0 or 128 floats
+    a->tmul[0] = 128;
+    gdim[1] = 128;  // columns: qubits 7..13
+    gstride[0] = 8ull << 7;
+    box[1] = 128;
+    gdim[2] = 1ull << (n - 14);  // qubits 14..n-1: tile bits 1..
+    gstride[1] = 8ull << 14;
+    box[2] = 1;
+    a->tshift[2] = 1;
+    a->tmaskc[2] = (uint32_t)((1ull << (n - 14)) - 1);
+    const CUresult r = encode(&a->tmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, amps, gdim, gstride, box, estr,
+                              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r == CUDA_SUCCESS) {
+      a->trank = 3;
+      a->tbytes = 132 * 128 * 4;
+    }
+    return;
+  }
   box[0] = 256;
-  a->tshift[0] = a->tmaskc[0] = 0;
   uint32_t rank = 1, tbit = 0;
   for (uint32_t q = 7; q < n;) {
     const bool blockq = (bmask >> q) & 1;
@@ -713,12 +761,14 @@ void set_tensor_map(uint32_t n, void* amps, BlockArgs* a) {
     ++rank;
     q += len;
   }
-  for (uint32_t d = rank; d < 5; ++d) a->tshift[d] = a->tmaskc[d] = 0;
   if (rank < 2) return;
   const CUresult r = encode(&a->tmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, rank, amps, gdim, gstride, box, estr,
                             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  if (r == CUDA_SUCCESS) a->trank = rank;
+  if (r == CUDA_SUCCESS) {
+    a->trank = rank;
+    a->tbytes = TILE_BYTES;
+  }
 }
 
 }  // namespace
