@@ -155,6 +155,7 @@ class TiledBlock:
 class Circuit:
     num_qubits: int
     instructions: list = field(default_factory=list)
+    num_clbits: int = 0
 
     def add(self, gate: Gate, qubits: Sequence[int], controls: Sequence[int] = ()) -> "Circuit":
         self.instructions.append(GateInstance(gate, qubits, controls))
