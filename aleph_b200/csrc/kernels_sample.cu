@@ -150,11 +150,20 @@ __global__ void alias_partition_kernel(uint64_t len, AliasScratch s) {
 // (descending stack order), and lane 0 runs the dependent chain out of
 // shared memory with the reference's operation order,
 //   alias[s] = l, threshold[s] = value(s), value(l) = (value(l) + value(s)) - 1.
-// status[0] is set on failure (never expected: the loop is bounded by 2N).
+// status[0] is set on failure (never expected: the rounds are bounded).
+// Lane 0's step is the add / subtract / compare and selects, without
+// data-dependent branches: the next entry of each buffer sits in registers one
+// step ahead (the buffers carry one spare slot so that this read never leaves
+// them), and each step's outputs (alias[s] = l, threshold[s]) go to a
+// shared-memory record ring that the whole warp scatters to global memory
+// when it fills or a buffer runs dry.
 constexpr int CHAIN_CH = 1024;
+constexpr int REC_CAP = 1024;
 __global__ void __launch_bounds__(32) alias_chain_kernel(uint64_t len, AliasScratch s, int32_t* status) {
-  __shared__ uint32_t sbi[CHAIN_CH], lbi[CHAIN_CH];
-  __shared__ double sbv[CHAIN_CH], lbv[CHAIN_CH];
+  __shared__ uint32_t sbi[CHAIN_CH + 1], lbi[CHAIN_CH + 1];
+  __shared__ double sbv[CHAIN_CH + 1], lbv[CHAIN_CH + 1];
+  __shared__ uint32_t rec_s[REC_CAP], rec_l[REC_CAP];
+  __shared__ double rec_v[REC_CAP];
   const int lane = threadIdx.x;
   if (len == 1) {
     if (lane == 0) {
@@ -195,36 +204,56 @@ __global__ void __launch_bounds__(32) alias_chain_kernel(uint64_t len, AliasScra
       pl = 0;
     }
     __syncwarp();
-    int done = 0;
+    int done = 0, nrec = 0;
     if (lane == 0) {
-      while (true) {
-        if (!hs && ps < ns) {
-          si = sbi[ps];
-          sv = sbv[ps];
-          ++ps;
-          hs = true;
-        }
-        if (!hl && pl < nl) {
-          li = lbi[pl];
-          lv = lbv[pl];
-          ++pl;
-          hl = true;
-        }
-        if (!hs || !hl) break;
-        if (++guard > 2 * len + 4) {
-          fail = 1;
-          break;
-        }
-        s.alias[si] = li;
-        s.prob[si] = sv;  // threshold = value of the small
-        const double r = __dsub_rn(__dadd_rn(lv, sv), 1.0);
-        if (r < 1.0) {  // the large becomes the next small
-          si = li;
-          sv = r;
-          hl = false;
-        } else {
-          lv = r;
-          hs = false;
+      if (++guard > 4 * (len / 256) + 64) fail = 1;  // rounds: refills plus ring flushes
+      if (!hs && ps < ns) {
+        si = sbi[ps];
+        sv = sbv[ps];
+        ++ps;
+        hs = true;
+      }
+      if (!hl && pl < nl) {
+        li = lbi[pl];
+        lv = lbv[pl];
+        ++pl;
+        hl = true;
+      }
+      if (hs && hl && !fail) {
+        // next entries of each buffer (meaningful while ps < ns / pl < nl)
+        uint32_t nsi = sbi[ps], nli = lbi[pl];
+        double nsv = sbv[ps], nlv = lbv[pl];
+        while (true) {
+          rec_s[nrec] = si;
+          rec_l[nrec] = li;
+          rec_v[nrec] = sv;  // threshold = value of the small
+          ++nrec;
+          const double r = __dsub_rn(__dadd_rn(lv, sv), 1.0);
+          const bool t = r < 1.0;  // the large becomes the next small
+          if (t ? pl >= nl : ps >= ns) {  // its successor is not buffered yet
+            if (t) {
+              si = li;
+              sv = r;
+              hl = false;
+            } else {
+              lv = r;
+              hs = false;
+            }
+            break;
+          }
+          const uint32_t si2 = t ? li : nsi, li2 = t ? nli : li;
+          const double sv2 = t ? r : nsv, lv2 = t ? nlv : r;
+          si = si2;
+          li = li2;
+          sv = sv2;
+          lv = lv2;
+          ps += t ? 0 : 1;
+          pl += t ? 1 : 0;
+          nsi = sbi[ps];
+          nsv = sbv[ps];
+          nli = lbi[pl];
+          nlv = lbv[pl];
+          if (nrec == REC_CAP) break;  // the warp flushes the ring first
         }
       }
       done = fail || (!hs && ps == ns && ts == 0) || (!hl && pl == nl && tl == 0);
@@ -232,6 +261,12 @@ __global__ void __launch_bounds__(32) alias_chain_kernel(uint64_t len, AliasScra
     ps = __shfl_sync(0xffffffffu, ps, 0);
     pl = __shfl_sync(0xffffffffu, pl, 0);
     done = __shfl_sync(0xffffffffu, done, 0);
+    nrec = __shfl_sync(0xffffffffu, nrec, 0);
+    __syncwarp();
+    for (int k = lane; k < nrec; k += 32) {  // scatter the step records
+      s.alias[rec_s[k]] = rec_l[k];
+      s.prob[rec_s[k]] = rec_v[k];
+    }
     __syncwarp();
     if (done) break;
   }
