@@ -1009,15 +1009,23 @@ int aleph_b200_sample(aleph_b200_handle* h, aleph_b200_state* st, uint32_t shots
   return ALEPH_B200_OK;
 }
 
+// Seeded sampling draws from the handle's own generator, so it is free to pick
+// the faster exact method: an alias table (one u64 per shot) while the
+// table's sequential construction is cheap (n <= 20, tens of ms), otherwise
+// the parallel inverse CDF (one f64 per shot), which also serves every n
+// above the alias limit of 28.
+constexpr uint32_t kSeededAliasMaxN = 20;
+
 int aleph_b200_sample_seeded(aleph_b200_handle* h, aleph_b200_state* st, uint32_t shots, uint64_t* out) {
   if (!h || !st || (shots && !out)) return ALEPH_B200_INVALID_ARGUMENT;
-  if (shots >= 2) {
+  if (shots >= 2 && st->n <= kSeededAliasMaxN) {
     std::vector<uint64_t> w(shots);
     for (auto& x : w) x = rng_next(h);
     return aleph_b200_sample(h, st, shots, ALEPH_B200_SAMPLE_ALIAS, w.data(), out);
   }
-  double u = shots ? rng_f64(h) : 0.0;
-  return aleph_b200_sample(h, st, shots, ALEPH_B200_SAMPLE_CUMULATIVE, &u, out);
+  std::vector<double> u(shots ? shots : 1, 0.0);
+  for (uint32_t k = 0; k < shots; ++k) u[k] = rng_f64(h);
+  return aleph_b200_sample(h, st, shots, ALEPH_B200_SAMPLE_CUMULATIVE, u.data(), out);
 }
 
 // ---- cumulative sampling from a fixed device buffer (no allocation) ------------

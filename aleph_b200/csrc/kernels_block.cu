@@ -410,7 +410,7 @@ __global__ void __launch_bounds__(blk::THREADS, 1) block_kernel(const __grid_con
       for (uint32_t r = lane; r < nruns; r += 32)
         bulk_load(dst0 + r * run_stride, a.amps + (base | runoff[r]), run_bytes, bar_sfull + 8 * s);
     }
-  } else if (warp < EPI_WARP0) {
+  } else if (warp >= CONV_WARP0 && warp < CONV_WARP0 + CONV_WARPS) {
     // ---------------- converters: stage -> BF16 hi/lo -> TMEM A operand ----------------
     const int q = warp & 3;  // TMEM lane quarter
     const int col = 32 * q + lane;

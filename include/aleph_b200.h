@@ -258,7 +258,9 @@ int aleph_b200_measure(aleph_b200_handle* h, aleph_b200_state* st, uint32_t qubi
  * `variates`: uint64 words (ALIAS) or doubles in [0,1) (CUMULATIVE), one per shot. */
 int aleph_b200_sample(aleph_b200_handle* h, aleph_b200_state* st, uint32_t shots, int mode, const void* variates,
                       uint64_t* out);
-/* Same, with variates drawn from the handle's RNG (AUTO rule). */
+/* Same, with variates drawn from the handle's RNG: ALIAS (one u64 per shot)
+ * for 2+ shots on n <= 20, otherwise CUMULATIVE (one double per shot), which
+ * covers every n, including those above the alias limit of 28. */
 int aleph_b200_sample_seeded(aleph_b200_handle* h, aleph_b200_state* st, uint32_t shots, uint64_t* out);
 
 /* CUMULATIVE sampling that allocates nothing. No counterpart in the reference.

@@ -297,6 +297,24 @@ def test_seeded_determinism():
     assert a.measure(sa, 3) == b.measure(sb, 3)
 
 
+@pytest.mark.parametrize("n,precision", [(22, "f64"), (29, "f32")])
+def test_seeded_sampling_beyond_the_alias_range(n, precision):
+    """Seeded sampling of many shots works for every n: above n = 20 it runs
+    the parallel inverse CDF (alias tables stop at n = 28)."""
+    c = C.Circuit(n).add(C.H(), [0])
+    for q in range(n - 1):
+        c.add(C.Cnot(), [q, q + 1])
+    outs = []
+    for _ in range(2):
+        be = B200SvBackend(seed=5, precision=precision)
+        st = run(be, c)
+        outs.append(be.sample(st, 1024))
+        be.close()
+    assert np.array_equal(outs[0], outs[1])
+    vals, cnt = np.unique(outs[0], return_counts=True)
+    assert set(int(v) for v in vals) == {0, (1 << n) - 1} and min(cnt) > 400
+
+
 # ---- TC32: fused 6-qubit blocks on tcgen05 tensor cores, split-BF16x3 ---------
 TC_TOL = 1e-5  # per-amplitude, the FP32 tolerance; 1 - fidelity checked at 1e-6
 
