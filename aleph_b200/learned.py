@@ -334,19 +334,44 @@ def training_circuits(scale: int = 0, seed: int = 0):
 
 
 def heldout_circuits(n_brick: int = 28, n_grover_data: int = 14, seed: int = 1):
-    """Held-out evaluation: a depth-40 random brickwall and Grover (20 iterations)."""
+    """Held-out evaluation: a depth-40 random brickwall, Grover (20
+    iterations) and the textbook QFT on a product state (none of them in the
+    training set with these sizes and seeds)."""
     from . import workloads as W
 
     rng = np.random.default_rng(seed)
     return [("brickwall", n_brick, W.brickwall(n_brick, 40, seed=seed).instructions),
-            ("grover", 2 * n_grover_data - 2, W.grover(n_grover_data, int(rng.integers(1 << n_grover_data)), 20).instructions)]
+            ("grover", 2 * n_grover_data - 2, W.grover(n_grover_data, int(rng.integers(1 << n_grover_data)), 20).instructions),
+            ("qft", n_brick, W.qft_product(n_brick, seed=seed).instructions)]
+
+
+def evaluate(model_path, heldout_n: int = 28, heldout_grover: int = 14) -> list:
+    """The learned planner (autotuned: kept only if measured faster and
+    state-equal) against the greedy plan on the held-out circuits."""
+    evals = []
+    for prec in ("f64", "tc32"):
+        bq = B200SvBackend(seed=0, precision=prec)
+        mq = CostModel.load(bq, model_path)
+        planner = LearnedPlanner(mq)
+        for name, n, instr in heldout_circuits(heldout_n, heldout_grover):
+            scored = planner.score(n, instr, prec)
+            res = autotune(bq, n, instr, planner, top_k=2)
+            evals.append({"precision": prec, "circuit": name, "n": n,
+                          "greedy_ms": round(res.greedy_ms, 3), "learned_ms": round(res.chosen_ms, 3),
+                          "gain": round(res.greedy_ms / res.chosen_ms, 4), "choice": res.choice.__dict__,
+                          "top_predicted": [(s.choice.__dict__, round(s.predicted_ms, 2)) for s in scored[:3]],
+                          "rejected": [str(r[1]) for r in res.rejected]})
+        mq.free()
+        bq.close()
+    return evals
 
 
 def main(argv=None) -> int:
     """python -m aleph_b200.learned [--out PATH] [--epochs E]: collect pass
     timings on the GPU (f64, f32 and tc32 handles), train the cost model,
     evaluate the learned planner against the greedy plan on held-out circuits,
-    print one JSON summary and save the model."""
+    print one JSON summary and save the model. With --eval-only: the held-out
+    evaluation of the model at --out, without collecting or training."""
     import argparse
     import json
     import time
@@ -357,7 +382,11 @@ def main(argv=None) -> int:
     ap.add_argument("--scale", type=int, default=0)
     ap.add_argument("--heldout-n", type=int, default=28)
     ap.add_argument("--heldout-grover", type=int, default=14)
+    ap.add_argument("--eval-only", action="store_true")
     args = ap.parse_args(argv)
+    if args.eval_only:
+        print(json.dumps({"model": str(args.out), "heldout": evaluate(args.out, args.heldout_n, args.heldout_grover)}))
+        return 0
     t0 = time.perf_counter()
     Xs, ys = [], []
     circuits = training_circuits(args.scale)
@@ -380,21 +409,7 @@ def main(argv=None) -> int:
     val_rmse = float(np.sqrt(np.mean((pred - y[val]) ** 2)))
     base_rmse = float(np.sqrt(np.mean((y[val] - y[~val].mean()) ** 2)))
     model.save(args.out)
-    evals = []
-    for prec in ("f64", "tc32"):
-        bq = B200SvBackend(seed=0, precision=prec)
-        mq = CostModel.load(bq, args.out)
-        planner = LearnedPlanner(mq)
-        for name, n, instr in heldout_circuits(args.heldout_n, args.heldout_grover):
-            scored = planner.score(n, instr, prec)
-            res = autotune(bq, n, instr, planner, top_k=2)
-            evals.append({"precision": prec, "circuit": name, "n": n,
-                          "greedy_ms": round(res.greedy_ms, 3), "learned_ms": round(res.chosen_ms, 3),
-                          "gain": round(res.greedy_ms / res.chosen_ms, 4), "choice": res.choice.__dict__,
-                          "top_predicted": [(s.choice.__dict__, round(s.predicted_ms, 2)) for s in scored[:3]],
-                          "rejected": [str(r[1]) for r in res.rejected]})
-        mq.free()
-        bq.close()
+    evals = evaluate(args.out, args.heldout_n, args.heldout_grover)
     print(json.dumps({"samples": int(len(y)), "circuits": len(circuits), "collect_s": round(t_collect, 1),
                       "train_s": round(t_train, 2), "train_samples_per_s": round(args.epochs * (~val).sum() / t_train),
                       "final_batch_loss": loss, "val_rmse_log": val_rmse, "val_rmse_mean_predictor": base_rmse,
