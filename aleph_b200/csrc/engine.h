@@ -71,6 +71,10 @@ struct BlockPass {
   uint32_t bq[6];
   uint32_t mat;        // offset of the split BF16 operand images in the block pool (bytes)
   uint32_t pre_begin, pre_count, post_begin, post_count;
+  // some post op is a phase that folds into per-column factors (a corner
+  // phase with at most one block qubit, or a one-qubit diagonal on a
+  // non-block qubit with no block controls): the kernel variant that folds
+  uint32_t fold;
 };
 
 // Kind 6 is the renormalisation that follows a tensor-core stream (pass records only).

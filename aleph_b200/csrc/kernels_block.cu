@@ -44,6 +44,7 @@
 
 #include <cstdint>
 #include <cstring>
+#include <type_traits>
 
 #include <cuda.h>  // CUtensorMap and its enums (the encoder is fetched through the runtime)
 #include <cuda_bf16.h>
@@ -288,6 +289,9 @@ struct BlockArgs {
   uint64_t runoff[128];  // global offset of run r
 };
 
+// FOLD: the variant for passes whose post ops include foldable phases
+// (BlockPass::fold); the plain variant keeps them out of its epilogue.
+template <bool FOLD>
 __global__ void __launch_bounds__(blk::THREADS, 1) block_kernel(const __grid_constant__ BlockArgs a) {
   using namespace blk;
   extern __shared__ uint8_t smem_raw[];
@@ -306,8 +310,15 @@ __global__ void __launch_bounds__(blk::THREADS, 1) block_kernel(const __grid_con
   __shared__ uint32_t tmem_base_sh;
   __shared__ int abort_sh;
   __shared__ uint64_t neg_rows[MAX_POST], neg_cmask[MAX_POST];
+  // Folded post phases: active for a column when (column & fold_cmask) ==
+  // fold_cmask; the factor (fold_c1 when column qubit fold_col is 1, else
+  // fold_c0) multiplies the rows whose block bit fold_rbit is set (all rows
+  // when fold_rbit < 0).
+  __shared__ uint64_t fold_cmask[MAX_POST];
+  __shared__ int8_t fold_rbit[MAX_POST], fold_col[MAX_POST];
+  __shared__ float2 fold_c0[MAX_POST], fold_c1[MAX_POST];
   __shared__ Op other_ops[MAX_POST];
-  __shared__ int n_neg_sh, n_other_sh;
+  __shared__ int n_neg_sh, n_other_sh, n_fold_sh;
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const uint32_t n = a.n;
@@ -335,7 +346,7 @@ __global__ void __launch_bounds__(blk::THREADS, 1) block_kernel(const __grid_con
     }
     fence_barrier_init();
     abort_sh = 0;
-    int nn = 0, no = 0;
+    int nn = 0, no = 0, nf = 0;
     const uint32_t cnt = a.post_count < (uint32_t)MAX_POST ? a.post_count : (uint32_t)MAX_POST;
     for (uint32_t o = 0; o < cnt; ++o) {
       const Op op = a.post[o];
@@ -350,12 +361,32 @@ __global__ void __launch_bounds__(blk::THREADS, 1) block_kernel(const __grid_con
         neg_rows[nn] = rows;
         neg_cmask[nn] = op.mask & ~bmask;
         ++nn;
+      } else if (FOLD && op.type == OP_CPHASE && __popcll(op.mask & bmask) <= 1) {
+        // a phase on a corner: at most one block qubit, the rest a column condition
+        const uint64_t rm = op.mask & bmask;
+        int rb = -1;
+        for (int b = 0; b < 6; ++b)
+          if (rm == (1ull << a.bq[b])) rb = b;
+        fold_cmask[nf] = op.mask & ~bmask;
+        fold_rbit[nf] = (int8_t)rb;
+        fold_col[nf] = -1;
+        fold_c0[nf] = fold_c1[nf] = a.coef[op.coef];
+        ++nf;
+      } else if (FOLD && op.type == OP_DIAG && op.nq == 1 && !((bmask >> op.q[0]) & 1) && !(op.ctrl & bmask)) {
+        // a one-qubit diagonal on a column qubit (controls on columns too)
+        fold_cmask[nf] = op.ctrl;
+        fold_rbit[nf] = -1;
+        fold_col[nf] = (int8_t)op.q[0];
+        fold_c0[nf] = a.coef[op.coef];
+        fold_c1[nf] = a.coef[op.coef + 1];
+        ++nf;
       } else {
         other_ops[no++] = op;
       }
     }
     n_neg_sh = nn;
     n_other_sh = no;
+    n_fold_sh = nf;
   }
   if (warp == 0) {
     tmem_alloc(smem_u32(&tmem_base_sh), TMEM_COLS);
@@ -497,7 +528,7 @@ __global__ void __launch_bounds__(blk::THREADS, 1) block_kernel(const __grid_con
     const int h = (warp - EPI_WARP0) >> 2;  // block rows 32h .. 32h+31
     const int col = 32 * q + lane;
     const bool pairs = a.bq[0] == 0;
-    const int n_neg = n_neg_sh, n_other = n_other_sh;
+    const int n_neg = n_neg_sh, n_other = n_other_sh, n_fold = n_fold_sh;
     uint32_t i = 0;
     for (uint64_t t = first; t < ntiles; t += stride, ++i) {
       const uint32_t b = i & 1, ph = (i >> 1) & 1;
@@ -505,6 +536,21 @@ __global__ void __launch_bounds__(blk::THREADS, 1) block_kernel(const __grid_con
       uint64_t neg = 0;
       for (int o = 0; o < n_neg; ++o)
         if ((gc & neg_cmask[o]) == neg_cmask[o]) neg ^= neg_rows[o];
+      // folded phases of this column: a factor for every row (fb) and one per
+      // block-row bit (fr[0..5])
+      float2 fb = make_float2(1.f, 0.f), fr[6];
+#pragma unroll
+      for (int r = 0; r < 6; ++r) fr[r] = make_float2(1.f, 0.f);
+      for (int o = 0; FOLD && o < n_fold; ++o) {
+        if ((gc & fold_cmask[o]) != fold_cmask[o]) continue;
+        const int cq = fold_col[o];
+        const float2 c = (cq >= 0 && ((gc >> cq) & 1)) ? fold_c1[o] : fold_c0[o];
+        const int rb = fold_rbit[o];
+        if (rb < 0) fb = cmul<float>(fb, c);
+#pragma unroll
+        for (int r = 0; r < 6; ++r)
+          if (rb == r) fr[r] = cmul<float>(fr[r], c);
+      }
       if (!mbar_wait(bar_dfull + 8 * b, ph, abort_flag)) {
         abort_sh = 1;
         break;
@@ -521,25 +567,40 @@ __global__ void __launch_bounds__(blk::THREADS, 1) block_kernel(const __grid_con
         if (lane == 0) mbar_arrive(bar_dempty + 8 * b);  // accumulator read: the MMA may reuse it
         const uint32_t negh = (uint32_t)(neg >> (32 * h));
         float2* pc = a.amps + gc;
+        // two copies of the row loop, so that passes without folded phases
+        // keep the plain one
+        auto store_rows = [&](auto fold_tag) {
+          constexpr bool WITH_FOLD = decltype(fold_tag)::value;
+          const float2 fh = h ? cmul<float>(fb, fr[5]) : fb;  // row bit 5 is this warp's half
 #pragma unroll
-        for (int jj = 0; jj < 32; jj += 2) {
-          float2 y0 = make_float2(re[jj], im[jj]), y1 = make_float2(re[jj + 1], im[jj + 1]);
-          if ((negh >> jj) & 1) y0 = make_float2(-y0.x, -y0.y);
-          if ((negh >> (jj + 1)) & 1) y1 = make_float2(-y1.x, -y1.y);
-          const uint64_t g0 = h ? a.grow[32 + jj] : a.grow[jj];
-          const uint64_t g1 = h ? a.grow[33 + jj] : a.grow[jj + 1];
-          if (n_other)
-            for (int o = 0; o < n_other; ++o) {
-              y0 = apply_diag_op<float>(other_ops[o], y0, gc | g0, a.coef, a.poly);
-              y1 = apply_diag_op<float>(other_ops[o], y1, gc | g1, a.coef, a.poly);
+          for (int jj = 0; jj < 32; jj += 2) {
+            float2 y0 = make_float2(re[jj], im[jj]), y1 = make_float2(re[jj + 1], im[jj + 1]);
+            if ((negh >> jj) & 1) y0 = make_float2(-y0.x, -y0.y);
+            if ((negh >> (jj + 1)) & 1) y1 = make_float2(-y1.x, -y1.y);
+            if constexpr (WITH_FOLD) {
+              float2 f0 = fh;
+#pragma unroll
+              for (int r = 1; r < 5; ++r)
+                if ((jj >> r) & 1) f0 = cmul<float>(f0, fr[r]);
+              y0 = cmul<float>(f0, y0);
+              y1 = cmul<float>(cmul<float>(f0, fr[0]), y1);  // row jj + 1 adds bit 0
             }
-          if (pairs) {
-            __stcs((float4*)(pc + g0), make_float4(y0.x, y0.y, y1.x, y1.y));
-          } else {
-            __stcs(pc + g0, y0);
-            __stcs(pc + g1, y1);
+            const uint64_t g0 = h ? a.grow[32 + jj] : a.grow[jj];
+            const uint64_t g1 = h ? a.grow[33 + jj] : a.grow[jj + 1];
+            if (n_other)
+              for (int o = 0; o < n_other; ++o) {
+                y0 = apply_diag_op<float>(other_ops[o], y0, gc | g0, a.coef, a.poly);
+                y1 = apply_diag_op<float>(other_ops[o], y1, gc | g1, a.coef, a.poly);
+              }
+            if (pairs) {
+              __stcs((float4*)(pc + g0), make_float4(y0.x, y0.y, y1.x, y1.y));
+            } else {
+              __stcs(pc + g0, y0);
+              __stcs(pc + g1, y1);
+            }
           }
-        }
+        };
+        store_rows(std::integral_constant<bool, FOLD>{});
       }
     }
   }
@@ -793,13 +854,18 @@ cudaError_t launch_block_pass(void* amps, const BlockPass& p, const uint8_t* ima
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   if (dev >= 64 || !((attr_devices >> dev) & 1)) {
-    e = cudaFuncSetAttribute(block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, blk::SMEM_BYTES);
+    e = cudaFuncSetAttribute(block_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, blk::SMEM_BYTES);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(block_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, blk::SMEM_BYTES);
     if (e != cudaSuccess) return e;
     if (dev < 64) attr_devices |= 1ull << dev;
   }
   const uint64_t ntiles = 1ull << (p.n - 13);
   const unsigned grid = (unsigned)(ntiles < (uint64_t)sm_count ? ntiles : (uint64_t)sm_count);
-  block_kernel<<<grid, blk::THREADS, blk::SMEM_BYTES, s>>>(a);
+  if (p.fold)
+    block_kernel<true><<<grid, blk::THREADS, blk::SMEM_BYTES, s>>>(a);
+  else
+    block_kernel<false><<<grid, blk::THREADS, blk::SMEM_BYTES, s>>>(a);
   return cudaGetLastError();
 }
 

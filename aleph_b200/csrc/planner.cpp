@@ -847,6 +847,13 @@ int plan_segment_blocks(const std::vector<const Lowered*>& seg, uint32_t n, uint
     ps.block.post_begin = (uint32_t)P->ops.size();
     for (const Lowered* L : post) append_op(P, *L, L->op);
     ps.block.post_count = (uint32_t)P->ops.size() - ps.block.post_begin;
+    ps.block.fold = 0;
+    for (const Lowered* L : post) {
+      const Op& op = L->op;
+      if ((op.type == OP_CPHASE && __builtin_popcountll(op.mask & B) <= 1) ||
+          (op.type == OP_DIAG && op.nq == 1 && !((B >> op.q[0]) & 1) && !(op.ctrl & B)))
+        ps.block.fold = 1;
+    }
     ps.record = take.front()->record;
     ps.gates = (uint32_t)(take.size() + post.size());
     count_ops(take, &ps);
