@@ -378,12 +378,13 @@ def qaoa_sweep_bench(dev: int, sets: int, loop_sample: int, seed: int) -> dict:
     return out
 
 
-def small_configs_bench(dev: int, seed: int) -> dict:
+def small_configs_bench(dev: int, seed: int, greedy: bool = False) -> dict:
     """The two plain-FP64 configurations beside the headline:
     C0: brickwall n=20 depth 20, full state and 1024 shots against the oracle;
     C1: textbook QFT (with bit-reversal swaps) on a random Ry.Rz product state
     at n=30: time, ||psi||^2 and 4096 shots on the device, and max|dpsi|
-    against the oracle on the n=24 copy of the circuit."""
+    against the oracle on the n=24 copy of the circuit. C1 runs the plan
+    configuration the committed cost model ranks first (unless ``greedy``)."""
     import torch
 
     from aleph_b200 import workloads
@@ -422,6 +423,16 @@ def small_configs_bench(dev: int, seed: int) -> dict:
     st.free()
 
     c1 = workloads.qft_product(30, seed=seed)
+    choice = None
+    if not greedy:
+        from aleph_b200 import learned
+
+        if learned.MODEL_PATH.exists():  # the learned plan, kept only if measured faster and state-equal
+            model = learned.CostModel.load(be, learned.MODEL_PATH)
+            try:
+                choice = learned.autotune(be, 30, c1.instructions, learned.LearnedPlanner(model), top_k=2).choice
+            finally:
+                model.free()
     st, ms = timed(30, c1)
     norm = be.norm_sqr(st)
     u = np.random.default_rng(seed).random(4096)
@@ -434,6 +445,7 @@ def small_configs_bench(dev: int, seed: int) -> dict:
     be.apply_stream(st24, c1s.instructions)
     w24, _ = oracle.run(24, c1s.instructions)
     out["c1_qft_n30"] = {"ms": round(ms, 3), "norm_sqr": norm, "shots_4096_ms": round(shots_ms, 2),
+                         "plan_choice": None if choice is None else dict(choice.__dict__, source="learned cost model, autotuned"),
                          "shots_mode": "cumulative (alias tables are built up to n=28)",
                          "n24_copy_max_abs_dpsi": float(np.abs(be.statevector(st24) - w24).max())}
     st24.free()
@@ -544,7 +556,7 @@ def run_engine(args, ranks: Ranks):
         qaoa = qaoa_sweep_bench(dev, args.qaoa_sets, 8, args.seed)
     small = None
     if not args.skip_small and ranks.rank == 0:
-        small = small_configs_bench(dev, args.seed)
+        small = small_configs_bench(dev, args.seed, greedy=args.greedy)
 
     cpu = None
     if ranks.world == 1 and not args.skip_cpu:

@@ -213,6 +213,13 @@ def test_swaps_relabel_into_permutation_passes():
     assert kinds(20, [sw(0, 1), sw(1, 2)]) == ["permute", "permute"]
     assert kinds(20, [sw(3, 17), sw(17, 3)]) == []
     assert kinds(20, [sw(3, 17)]) == ["permute"]
+    # any relabeling settles in at most two involution passes: a 20-cycle, a
+    # 5-cycle beside disjoint transpositions, and a product of disjoint swaps
+    cycle = [sw(q, q + 1) for q in range(19)]
+    assert kinds(20, cycle) == ["permute", "permute"]
+    mixed = [sw(0, 1), sw(1, 2), sw(2, 3), sw(3, 4), sw(10, 11), sw(12, 19)]
+    assert kinds(20, mixed) == ["permute", "permute"]
+    assert kinds(20, [sw(0, 19), sw(5, 6), sw(8, 13)]) == ["permute"]
     # a controlled SWAP is a gate; so is any SWAP of a state that fits one shared-memory pass
     assert kinds(20, [sw(3, 17, [5])]) == ["tile"]
     assert kinds(12, [sw(3, 7)]) == ["smem"]
