@@ -82,7 +82,9 @@ constexpr int OFF_S = OFF_W + W_BYTES;                    // two FP32 input stag
 constexpr int OFF_TAB = OFF_S + 2 * STAGE_BYTES;          // lane-indexed tables
 constexpr int TAB_BYTES = NCOL * 4 + NCOL * 8 + MAX_RUNS * 8;
 constexpr int OFF_BAR = OFF_TAB + TAB_BYTES;              // mbarriers
-constexpr int SMEM_BYTES = OFF_BAR + 128 + 1024;          // + alignment slack
+constexpr int EPI_STAGE_BYTES = 32 * 8 * 8;               // per epilogue warp: 32 columns x 8 rows
+constexpr int OFF_EPI = OFF_BAR + 128;                    // epilogue transposes (blocks on qubits 0..2)
+constexpr int SMEM_BYTES = OFF_EPI + EPI_WARPS * EPI_STAGE_BYTES + 1024;  // + alignment slack
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -319,6 +321,10 @@ __global__ void __launch_bounds__(blk::THREADS, 1) block_kernel(const __grid_con
   __shared__ float2 fold_c0[MAX_POST], fold_c1[MAX_POST];
   __shared__ Op other_ops[MAX_POST];
   __shared__ int n_neg_sh, n_other_sh, n_fold_sh;
+  // The non-tile qubits as runs of consecutive positions: tile index bits
+  // [dep_src, dep_src + len) land on qubits [dep_dst, dep_dst + len).
+  __shared__ uint32_t dep_src[16], dep_mask[16], dep_dst[16];
+  __shared__ int n_dep_sh;
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const uint32_t n = a.n;
@@ -346,6 +352,22 @@ __global__ void __launch_bounds__(blk::THREADS, 1) block_kernel(const __grid_con
     }
     fence_barrier_init();
     abort_sh = 0;
+    int nd = 0;
+    for (uint32_t q = 0, src = 0; q < n;) {
+      if ((tmask >> q) & 1) {
+        ++q;
+        continue;
+      }
+      uint32_t len = 0;
+      while (q + len < n && !((tmask >> (q + len)) & 1)) ++len;
+      dep_src[nd] = src;
+      dep_mask[nd] = (1u << len) - 1;  // len <= n - 13 <= 27
+      dep_dst[nd] = q;
+      ++nd;
+      src += len;
+      q += len;
+    }
+    n_dep_sh = nd;  // at most 14: the 13 tile qubits leave at most 14 gaps
     int nn = 0, no = 0, nf = 0;
     const uint32_t cnt = a.post_count < (uint32_t)MAX_POST ? a.post_count : (uint32_t)MAX_POST;
     for (uint32_t o = 0; o < cnt; ++o) {
@@ -398,13 +420,11 @@ __global__ void __launch_bounds__(blk::THREADS, 1) block_kernel(const __grid_con
   const uint32_t tmem = tmem_base_sh;
 
   const uint64_t ntiles = 1ull << (n - 13);
+  const int n_dep = n_dep_sh;
   auto tile_base = [&](uint64_t t) -> uint64_t {  // deposit a tile index into the non-tile qubits
+    const uint32_t tt = (uint32_t)t;              // n - 13 <= 27 bits
     uint64_t base = 0;
-    for (uint32_t q = 0; t != 0 && q < n; ++q) {
-      if ((tmask >> q) & 1) continue;
-      base |= (t & 1) << q;
-      t >>= 1;
-    }
+    for (int k = 0; k < n_dep; ++k) base |= (uint64_t)((tt >> dep_src[k]) & dep_mask[k]) << dep_dst[k];
     return base;
   };
   const uint64_t first = blockIdx.x, stride = gridDim.x;
@@ -528,11 +548,17 @@ __global__ void __launch_bounds__(blk::THREADS, 1) block_kernel(const __grid_con
     const int h = (warp - EPI_WARP0) >> 2;  // block rows 32h .. 32h+31
     const int col = 32 * q + lane;
     const bool pairs = a.bq[0] == 0;
+    // With qubits 0, 1, 2 as block bits 0..2, rows 8k .. 8k+7 of a column are
+    // 64 contiguous bytes in HBM: those tiles are written through a small
+    // per-warp shared-memory transpose (32 columns x 8 rows).
+    const bool octets = pairs && a.bq[1] == 1 && a.bq[2] == 2;
+    float4* ep = (float4*)(sm + OFF_EPI + EPI_STAGE_BYTES * (warp - EPI_WARP0));
     const int n_neg = n_neg_sh, n_other = n_other_sh, n_fold = n_fold_sh;
     uint32_t i = 0;
     for (uint64_t t = first; t < ntiles; t += stride, ++i) {
       const uint32_t b = i & 1, ph = (i >> 1) & 1;
-      const uint64_t gc = tile_base(t) | Gcol[col];
+      const uint64_t tb = tile_base(t);
+      const uint64_t gc = tb | Gcol[col];
       uint64_t neg = 0;
       for (int o = 0; o < n_neg; ++o)
         if ((gc & neg_cmask[o]) == neg_cmask[o]) neg ^= neg_rows[o];
@@ -567,10 +593,12 @@ __global__ void __launch_bounds__(blk::THREADS, 1) block_kernel(const __grid_con
         if (lane == 0) mbar_arrive(bar_dempty + 8 * b);  // accumulator read: the MMA may reuse it
         const uint32_t negh = (uint32_t)(neg >> (32 * h));
         float2* pc = a.amps + gc;
-        // two copies of the row loop, so that passes without folded phases
-        // keep the plain one
-        auto store_rows = [&](auto fold_tag) {
+        // separate copies of the row loop, so that passes without folded
+        // phases or general post ops keep the plain one
+        auto store_rows = [&](auto fold_tag, auto other_tag, auto octet_tag) {
           constexpr bool WITH_FOLD = decltype(fold_tag)::value;
+          constexpr bool WITH_OTHER = decltype(other_tag)::value;
+          constexpr bool OCTETS = decltype(octet_tag)::value;
           const float2 fh = h ? cmul<float>(fb, fr[5]) : fb;  // row bit 5 is this warp's half
 #pragma unroll
           for (int jj = 0; jj < 32; jj += 2) {
@@ -587,12 +615,41 @@ __global__ void __launch_bounds__(blk::THREADS, 1) block_kernel(const __grid_con
             }
             const uint64_t g0 = h ? a.grow[32 + jj] : a.grow[jj];
             const uint64_t g1 = h ? a.grow[33 + jj] : a.grow[jj + 1];
-            if (n_other)
-              for (int o = 0; o < n_other; ++o) {
-                y0 = apply_diag_op<float>(other_ops[o], y0, gc | g0, a.coef, a.poly);
-                y1 = apply_diag_op<float>(other_ops[o], y1, gc | g1, a.coef, a.poly);
+            if constexpr (WITH_OTHER) {
+              // general post ops (rare): stage this thread's 8-row chunk in
+              // its own slots of the warp's buffer, then apply them in a
+              // rolled loop and store from there
+              float2* eo = (float2*)ep;  // [row in chunk][lane]
+              eo[(jj & 7) * 32 + lane] = y0;
+              eo[((jj & 7) + 1) * 32 + lane] = y1;
+              if ((jj & 7) == 6) {
+                const int j0 = 32 * h + (jj & ~7);
+#pragma unroll 1
+                for (int r = 0; r < 8; ++r) {
+                  float2 y = eo[r * 32 + lane];
+                  const uint64_t g = a.grow[j0 + r];
+                  for (int o = 0; o < n_other; ++o) y = apply_diag_op<float>(other_ops[o], y, gc | g, a.coef, a.poly);
+                  __stcs(pc + g, y);
+                }
               }
-            if (pairs) {
+            } else if constexpr (OCTETS) {
+              // stage the row pair; after every 8 rows the warp writes them
+              // out column by column, 64 contiguous bytes per column (8 lines
+              // per store instruction instead of 32)
+              ep[4 * lane + (((jj & 7) >> 1) ^ ((lane >> 1) & 3))] = make_float4(y0.x, y0.y, y1.x, y1.y);
+              if ((jj & 7) == 6) {
+                __syncwarp();
+                const uint64_t gr = h ? a.grow[32 + (jj & ~7)] : a.grow[jj & ~7];
+                const int qd = lane & 3;
+#pragma unroll
+                for (int m = 0; m < 4; ++m) {
+                  const int c = 8 * m + (lane >> 2);
+                  const float4 v = ep[4 * c + (qd ^ ((c >> 1) & 3))];
+                  __stcs((float4*)(a.amps + ((tb | Gcol[32 * q + c]) + gr + 2 * qd)), v);
+                }
+                __syncwarp();
+              }
+            } else if (pairs) {
               __stcs((float4*)(pc + g0), make_float4(y0.x, y0.y, y1.x, y1.y));
             } else {
               __stcs(pc + g0, y0);
@@ -600,7 +657,12 @@ __global__ void __launch_bounds__(blk::THREADS, 1) block_kernel(const __grid_con
             }
           }
         };
-        store_rows(std::integral_constant<bool, FOLD>{});
+        if (n_other)
+          store_rows(std::integral_constant<bool, FOLD>{}, std::true_type{}, std::false_type{});
+        else if (octets)
+          store_rows(std::integral_constant<bool, FOLD>{}, std::false_type{}, std::true_type{});
+        else
+          store_rows(std::integral_constant<bool, FOLD>{}, std::false_type{}, std::false_type{});
       }
     }
   }

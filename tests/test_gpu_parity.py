@@ -12,7 +12,7 @@ import pytest
 
 from aleph_b200 import circuit as C
 from aleph_b200 import workloads
-from aleph_b200.backend import B200SvBackend, run, run_with_outcomes
+from aleph_b200.backend import B200SvBackend, describe_plan, run, run_with_outcomes
 from oracle import oracle
 from tests.fixtures_util import fixture_instructions, fixture_state, load_reference_fixtures
 
@@ -381,6 +381,60 @@ def test_compiled_plan_matches_stream(precision):
     with pytest.raises(Exception):
         plan.execute(st, [0.5])
     plan.free()
+
+
+BLOCK_LAYOUTS = {
+    "octets": [0, 1, 2, 3, 4, 5],      # rows 8k..8k+7 adjacent: staged transpose on store
+    "pairs": [0, 3, 5, 8, 9, 11],      # rows 2p, 2p+1 adjacent: 16-byte stores
+    "plain": [7, 8, 9, 10, 11, 12],    # one 8-byte store per row
+}
+
+
+@pytest.mark.parametrize("post", ["signs", "folded", "general"])
+@pytest.mark.parametrize("layout", sorted(BLOCK_LAYOUTS))
+def test_tc32_block_epilogue_paths(layout, post):
+    """Every store path of the block epilogue against the oracle, with each
+    kind of diagonal op after the block: sign flips (CZ), phases folded into
+    per-column factors (controlled phases with at most one block qubit,
+    one-qubit diagonals on column qubits) and the general route (two-qubit
+    diagonals across the block, phase polynomials)."""
+    n = 16
+    bq = BLOCK_LAYOUTS[layout]
+    out = [q for q in range(n) if q not in bq]
+    rng = np.random.default_rng(7)
+    psi0 = rng.normal(size=1 << n) + 1j * rng.normal(size=1 << n)
+    psi0 /= np.linalg.norm(psi0)
+    c = C.Circuit(n)
+    for _ in range(2):
+        for q in bq:
+            c.add(C.Unitary1q(workloads.haar_su2(rng)), [q])
+        for a, b in zip(bq, bq[1:]):
+            c.add(C.Cz(), [a, b])
+    ph = np.exp(1j * rng.uniform(0, 2 * np.pi, 4))
+    if post == "signs":
+        c.add(C.Cz(), [bq[1], out[-1]]).add(C.Cz(), [out[0], out[-2]]).add(C.Cz(), [bq[0], bq[4]])
+    elif post == "folded":
+        c.add(C.Unitary2qDiag([1, 1, 1, ph[0]]), [bq[2], out[-1]])
+        c.add(C.Unitary2qDiag([1, 1, 1, ph[1]]), [out[1], out[-3]])
+        c.add(C.Phase(0.37), [out[-2]]).add(C.Rz(0.91), [out[2]])
+    else:
+        c.add(C.Unitary2qDiag(ph), [bq[0], out[-1]])
+        c.add(C.Rz(0.7), [bq[3]], controls=[out[-2]])
+        c.instructions.append(C.DiagonalPhase(n, [C.PhaseTerm((1 << bq[1] | 1 << out[0],), 0.43),
+                                                  C.PhaseTerm((1 << bq[5], 1 << out[3]), -1.1)]))
+        c.add(C.Cz(), [bq[2], out[-3]])
+    plan = describe_plan(n, c.instructions, precision="tc32")
+    assert plan[0]["kind"] == "block" and plan[0]["qubits"] == bq and plan[0]["post_ops"] > 0
+    be = B200SvBackend(seed=0, precision="tc32")
+    st = be.allocate(n)
+    be.set_statevector(st, psi0)
+    be.apply_stream(st, c.instructions)
+    got = be.statevector(st)
+    want, _ = oracle.run(n, c.instructions, state=psi0)
+    assert be.stats()["block_passes"] > 0
+    assert np.abs(got - want).max() <= TC_TOL
+    assert 1.0 - fidelity(got, want) <= 1e-6
+    be.close()
 
 
 @pytest.mark.parametrize("window_search", [0, 1])
