@@ -192,6 +192,9 @@ _SIGNATURES = {
     "aleph_b200_expectation": (
         [_P, _P, ct.POINTER(ct.c_uint32), ct.POINTER(ct.c_uint8), ct.c_uint32, ct.c_double,
          ct.POINTER(ct.c_double)], ct.c_int),
+    "aleph_b200_expectation_sum": (
+        [_P, _P, ct.POINTER(ct.c_uint32), ct.POINTER(ct.c_uint8), ct.POINTER(ct.c_uint64), ct.POINTER(ct.c_double),
+         ct.c_uint64, ct.POINTER(ct.c_double), ct.POINTER(ct.c_double)], ct.c_int),
     "aleph_b200_probabilities": ([_P, _P, ct.POINTER(ct.c_uint32), ct.c_uint32, ct.POINTER(ct.c_double)], ct.c_int),
     "aleph_b200_get_amplitudes": ([_P, _P, ct.POINTER(ct.c_double)], ct.c_int),
     "aleph_b200_set_amplitudes": ([_P, _P, ct.POINTER(ct.c_double)], ct.c_int),

@@ -178,6 +178,30 @@ class B200SvBackend:
                                                     ct.byref(out)))
         return out.value
 
+    def expectation_sum(self, state: State, terms, with_terms: bool = False):
+        """``expectation_pauli_sum`` (crates/aleph-backend/src/lib.rs:422-432):
+        ``terms`` is a sequence of (coefficient, [(qubit, 'I'|'X'|'Y'|'Z'), ...]).
+        Returns the sum, or (sum, per-term values) with ``with_terms``."""
+        k = len(terms)
+        offsets = [0]
+        qs, ps = [], []
+        for _, string in terms:
+            for q, p in string:
+                qs.append(int(q))
+                ps.append(abi.PAULI[p])
+            offsets.append(len(qs))
+        cq = (ct.c_uint32 * max(1, len(qs)))(*qs)
+        cp = (ct.c_uint8 * max(1, len(ps)))(*ps)
+        co = (ct.c_uint64 * (k + 1))(*offsets)
+        cc = (ct.c_double * max(1, k))(*[float(c) for c, _ in terms])
+        vals = (ct.c_double * max(1, k))()
+        out = ct.c_double()
+        self._check(self.lib.aleph_b200_expectation_sum(self.handle, state.ptr, cq, cp, co, cc, k, ct.byref(out),
+                                                        vals if with_terms else None))
+        if with_terms:
+            return out.value, np.array(vals[:k], dtype=np.float64)
+        return out.value
+
     def probabilities(self, state: State, qubits) -> np.ndarray:
         k = len(qubits)
         qs = (ct.c_uint32 * max(1, k))(*qubits)

@@ -13,6 +13,7 @@
 #include <cstring>
 #include <mutex>
 #include <new>
+#include <unordered_map>
 #include <vector>
 
 #include "engine.h"
@@ -1160,6 +1161,117 @@ int aleph_b200_expectation(aleph_b200_handle* h, aleph_b200_state* st, const uin
   }
   if (bad_pauli) return set_error(h, ALEPH_B200_INVALID_ARGUMENT, "unknown Pauli code");
   *out = coefficient * res[2];
+  return ALEPH_B200_OK;
+}
+
+int aleph_b200_expectation_sum(aleph_b200_handle* h, aleph_b200_state* st, const uint32_t* qubits,
+                               const uint8_t* paulis, const uint64_t* offsets, const double* coefficients,
+                               uint64_t n_terms, double* out, double* term_values) {
+  if (!h || !st || !out || (n_terms && (!offsets || !coefficients))) return ALEPH_B200_INVALID_ARGUMENT;
+  for (uint64_t k = 0; k < n_terms; ++k)
+    if (offsets[k + 1] < offsets[k]) return set_error(h, ALEPH_B200_INVALID_ARGUMENT, "term offsets decrease");
+  if (n_terms && offsets[n_terms] > offsets[0] && (!qubits || !paulis)) return ALEPH_B200_INVALID_ARGUMENT;
+  if (int r = bind(h)) return r;
+  *out = 0.0;
+  if (n_terms == 0) return ALEPH_B200_OK;  // the reference's loop evaluates no term and validates nothing
+
+  // per-term masks, as aleph_b200_expectation forms them
+  struct TermMasks {
+    uint64_t xm = 0, zm = 0;
+    uint32_t ny = 0;
+    bool bad_pauli = false;
+  };
+  std::vector<TermMasks> tm(n_terms);
+  for (uint64_t k = 0; k < n_terms; ++k) {
+    TermMasks& m = tm[k];
+    bool in_range = true;
+    for (uint64_t t = offsets[k]; t < offsets[k + 1]; ++t) {
+      if (qubits[t] >= st->n) in_range = false;
+      if (qubits[t] >= 64) continue;
+      switch (paulis[t]) {
+        case ALEPH_PAULI_I: break;
+        case ALEPH_PAULI_X: m.xm |= 1ull << qubits[t]; break;
+        case ALEPH_PAULI_Y: m.xm |= 1ull << qubits[t]; m.zm |= 1ull << qubits[t]; ++m.ny; break;
+        case ALEPH_PAULI_Z: m.zm |= 1ull << qubits[t]; break;
+        default: m.bad_pauli = true;
+      }
+    }
+    if (!in_range) m.xm = m.zm = 0;  // evaluated as the identity; reported as out of range below
+  }
+  // group the terms by X/Y positions (first appearance order), chunks of MAX_TERMS
+  std::vector<PauliGroup> chunks;
+  std::vector<std::pair<uint32_t, uint32_t>> slot(n_terms);  // term -> (chunk, index in chunk)
+  {
+    std::unordered_map<uint64_t, uint32_t> open;  // xmask -> chunk still filling
+    for (uint64_t k = 0; k < n_terms; ++k) {
+      auto it = open.find(tm[k].xm);
+      if (it == open.end() || chunks[it->second].count == (uint32_t)PauliGroup::MAX_TERMS) {
+        PauliGroup g{};
+        g.xmask = tm[k].xm;
+        chunks.push_back(g);
+        open[tm[k].xm] = (uint32_t)(chunks.size() - 1);
+        it = open.find(tm[k].xm);
+      }
+      PauliGroup& g = chunks[it->second];
+      g.zmask[g.count] = tm[k].zm;
+      g.ny[g.count] = tm[k].ny;
+      slot[k] = {it->second, g.count};
+      ++g.count;
+    }
+  }
+  constexpr size_t NV = 2 + PauliGroup::MAX_TERMS;
+  const uint32_t nb = reduce_blocks(st->n, h->sm_count);
+  if (int r = ensure(h, h->reduce, ((size_t)nb + chunks.size()) * NV * 8 + 256)) return r;
+  double* part = (double*)h->reduce.ptr;
+  double* res = part + NV * (size_t)nb;
+  for (size_t c = 0; c < chunks.size(); ++c)
+    CK(launch_pauli_group(st->amps, st->precision, st->n, chunks[c], part, nb, res + NV * c, h->stream),
+       "Pauli sum");
+  h->stats.kernel_launches += 2 * chunks.size();
+  std::vector<double> host(NV * chunks.size());
+  CK(copy_async(h, host.data(), res, host.size() * 8, cudaMemcpyDeviceToHost, h->stream), "Pauli sum readback");
+  CK(cudaStreamSynchronize(h->stream), "stream synchronize");
+
+  // the reference sums expectation_value over the terms in order
+  // (crates/aleph-backend/src/lib.rs:422-432): the state is validated first
+  // (measure.rs:166), then each term's coefficient, qubits and duplicates in
+  // term order; the first failure is the error
+  const double len = (double)(1ull << st->n);
+  if (host[1] > 0.0 || !std::isfinite(host[0]) || std::fabs(host[0] - 1.0) > norm_tolerance((uint64_t)len, st->precision)) {
+    aleph_b200_error_info e{};
+    e.status = ALEPH_B200_INVALID_STATE;
+    std::snprintf(e.kind, sizeof(e.kind), "state norm2 deviates from 1");
+    return report(h, e);
+  }
+  double energy = 0.0;
+  for (uint64_t k = 0; k < n_terms; ++k) {
+    if (!std::isfinite(coefficients[k])) {
+      aleph_b200_error_info e{};
+      e.status = ALEPH_B200_INVALID_PAULI_STRING;
+      std::snprintf(e.kind, sizeof(e.kind), "non-finite coefficient");
+      return report(h, e);
+    }
+    for (uint64_t t = offsets[k]; t < offsets[k + 1]; ++t) {
+      aleph_b200_error_info e{};
+      if (qubits[t] >= st->n) {
+        e.status = ALEPH_B200_QUBIT_OUT_OF_RANGE;
+        e.qubit = qubits[t];
+        e.num_qubits = st->n;
+        return report(h, e);
+      }
+      for (uint64_t j = offsets[k]; j < t; ++j)
+        if (qubits[j] == qubits[t]) {
+          e.status = ALEPH_B200_DUPLICATE_QUBIT;
+          e.qubit = qubits[t];
+          return report(h, e);
+        }
+    }
+    if (tm[k].bad_pauli) return set_error(h, ALEPH_B200_INVALID_ARGUMENT, "unknown Pauli code");
+    const double v = coefficients[k] * host[NV * slot[k].first + 2 + slot[k].second];
+    if (term_values) term_values[k] = v;
+    energy += v;
+  }
+  *out = energy;
   return ALEPH_B200_OK;
 }
 

@@ -239,6 +239,18 @@ cudaError_t launch_measure_pass(void* amps, int precision, uint32_t n, uint32_t 
                                 uint8_t* outcome_slot, cudaStream_t s);
 cudaError_t launch_expectation(const void* amps, int precision, uint32_t n, uint64_t xmask, uint64_t zmask,
                                uint32_t ny, double* partials, uint32_t nblocks, double* out3, cudaStream_t s);
+// Up to MAX_TERMS Pauli strings with the same X/Y positions (xmask), each with
+// its Z/Y positions and number of Y factors: evaluated in one sweep.
+struct PauliGroup {
+  static constexpr int MAX_TERMS = 16;
+  uint64_t xmask;
+  uint32_t count;
+  uint64_t zmask[MAX_TERMS];
+  uint32_t ny[MAX_TERMS];
+};
+// out: [sum |a|^2, non-finite count, Re <P_0>, ..., Re <P_15>] (2 + MAX_TERMS doubles)
+cudaError_t launch_pauli_group(const void* amps, int precision, uint32_t n, const PauliGroup& g, double* partials,
+                               uint32_t nblocks, double* out, cudaStream_t s);
 cudaError_t launch_probabilities(const void* amps, int precision, uint32_t n, const uint32_t* qubits_dev, uint32_t k,
                                  double* partials, uint32_t nblocks, double* out, double* norm_out, cudaStream_t s);
 uint32_t reduce_blocks(uint32_t n, int sm_count);

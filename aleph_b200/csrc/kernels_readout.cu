@@ -230,6 +230,65 @@ cudaError_t launch_expectation(const void* amps, int precision, uint32_t n, uint
   return cudaGetLastError();
 }
 
+// ---- Pauli sum: up to 16 terms that share one X/Y (flip) mask, one sweep ----------
+// For every term: Re <psi|P|psi> with P as in expect_kernel. (P psi)_i differs
+// between the terms of a group only in the sign (-1)^{popc(zmask & j)} and the
+// factor i^ny, so conj(a_i) a_j is formed once per amplitude and shared.
+// partials per block: [sum |a|^2, non-finite count, term 0 .. 15].
+template <typename Real, bool DIAG>
+__global__ void __launch_bounds__(RB) pauli_group_kernel(const V2<Real>* __restrict__ amps, uint64_t len,
+                                                         const PauliGroup g, double* __restrict__ partials) {
+  double v[2 + PauliGroup::MAX_TERMS];
+#pragma unroll
+  for (int k = 0; k < 2 + PauliGroup::MAX_TERMS; ++k) v[k] = 0.0;
+  for (uint64_t i = (uint64_t)blockIdx.x * RB + threadIdx.x; i < len; i += (uint64_t)gridDim.x * RB) {
+    const V2<Real> a = ld_amp<Real>(amps + i);
+    const double p = abs2<Real>(a);
+    if (!isfinite(p)) {
+      v[1] += 1.0;
+      continue;
+    }
+    v[0] += p;
+    if constexpr (DIAG) {  // no X/Y factor: Re conj(a) a = |a|^2 and ny = 0
+#pragma unroll
+      for (int k = 0; k < PauliGroup::MAX_TERMS; ++k)
+        if (k < (int)g.count) v[2 + k] += (__popcll(g.zmask[k] & i) & 1) ? -p : p;
+    } else {
+      const uint64_t j = i ^ g.xmask;
+      const V2<Real> b = ld_amp<Real>(amps + j);
+      const double re = (double)a.x * b.x + (double)a.y * b.y;  // conj(a) * b
+      const double im = (double)a.x * b.y - (double)a.y * b.x;
+#pragma unroll
+      for (int k = 0; k < PauliGroup::MAX_TERMS; ++k)
+        if (k < (int)g.count) {
+          // i^ny: ny & 3 = 0, 1, 2, 3 keeps re, -im, -re, im
+          const uint32_t q = g.ny[k] & 3;
+          double t = (q & 1) ? im : re;
+          if ((q == 1 || q == 2) != (bool)(__popcll(g.zmask[k] & j) & 1)) t = -t;
+          v[2 + k] += t;
+        }
+    }
+  }
+  block_reduce_store<2 + PauliGroup::MAX_TERMS>(v, partials + (2 + PauliGroup::MAX_TERMS) * (size_t)blockIdx.x);
+}
+
+cudaError_t launch_pauli_group(const void* amps, int precision, uint32_t n, const PauliGroup& g, double* partials,
+                               uint32_t nblocks, double* out, cudaStream_t s) {
+  const uint64_t len = 1ull << n;
+  constexpr int NV = 2 + PauliGroup::MAX_TERMS;
+  if (g.count == 0 || g.count > (uint32_t)PauliGroup::MAX_TERMS) return cudaErrorInvalidValue;
+  const bool diag = g.xmask == 0;
+  if (precision == ALEPH_B200_F64) {
+    if (diag) pauli_group_kernel<double, true><<<nblocks, RB, 0, s>>>((const double2*)amps, len, g, partials);
+    else pauli_group_kernel<double, false><<<nblocks, RB, 0, s>>>((const double2*)amps, len, g, partials);
+  } else {
+    if (diag) pauli_group_kernel<float, true><<<nblocks, RB, 0, s>>>((const float2*)amps, len, g, partials);
+    else pauli_group_kernel<float, false><<<nblocks, RB, 0, s>>>((const float2*)amps, len, g, partials);
+  }
+  finish_kernel<NV><<<1, 32, 0, s>>>(partials, nblocks, out);
+  return cudaGetLastError();
+}
+
 // ---- marginal probabilities ------------------------------------------------------
 // k <= 10: per-block shared-memory histograms, summed by a second kernel.
 template <typename Real>

@@ -152,8 +152,8 @@ def run(circuit, *, shots: int = DEFAULT_SHOTS, backend: str = "b200", precision
 def qaoa_energy(n_qubits: int, edges, gammas, betas, backend: str = "b200", precision: str = "f64") -> float:
     """⟨H_C⟩ of QAOA Max-Cut (``build_qaoa`` + ``maxcut_pauli_sum``,
     crates/aleph-ir/src/ansatz.rs:71-117) at the given angles: one set of
-    the batched sweep kernel (n <= 26), or the gate stream plus one
-    ⟨Z_i Z_j⟩ reduction per edge beyond it."""
+    the batched sweep kernel (n <= 26), or the gate stream plus one fused
+    Pauli-sum expectation (every ⟨Z_i Z_j⟩ in shared sweeps) beyond it."""
     return float(qaoa_energies([(n_qubits, list(edges))], [gammas], [betas], backend, precision)[0])
 
 
@@ -182,7 +182,7 @@ def qaoa_energies(graphs, gammas, betas, backend: str = "b200", precision: str =
                 continue
             st = be.allocate(n)
             be.apply_stream(st, workloads.qaoa_maxcut(n, e, gammas[i], betas[i]).instructions)
-            out[i] = sum(0.5 * (1.0 - be.expectation_value(st, [(a, "Z"), (b, "Z")])) for a, b in e)
+            out[i] = be.expectation_sum(st, workloads.maxcut_pauli_sum(n, e))
             st.free()
         return out
     finally:

@@ -153,9 +153,16 @@ def grover(n_data: int, marked: int, iterations: int) -> C.Circuit:
     return c
 
 
-def maxcut_terms(edges):
-    """<C> = sum_edges 1/2 (1 - <Z_i Z_j>) (crates/aleph-ir/src/ansatz.rs:105-117)."""
-    return [((i, "Z"), (j, "Z")) for (i, j) in edges]
+def maxcut_pauli_sum(n: int, edges):
+    """``maxcut_pauli_sum`` (crates/aleph-ir/src/ansatz.rs:105-117): the
+    identity with coefficient |E|/2, then -1/2 Z_i Z_j per edge, as
+    (coefficient, [(qubit, letter), ...]) terms for ``expectation_sum``."""
+    terms = [(0.5 * len(edges), [])]
+    for (i, j) in edges:
+        if i >= n or j >= n:
+            raise ValueError(f"edge ({i}, {j}) out of range for {n} qubits")
+        terms.append((-0.5, [(i, "Z"), (j, "Z")]))
+    return terms
 
 
 def splitmix64_words(seed: int, count: int) -> np.ndarray:

@@ -13,6 +13,7 @@
  *   Backend::measure              -> aleph_b200_measure
  *   Backend::sample               -> aleph_b200_sample / aleph_b200_sample_seeded
  *   Backend::expectation_value    -> aleph_b200_expectation
+ *   expectation_pauli_sum         -> aleph_b200_expectation_sum
  *   Backend::probabilities        -> aleph_b200_probabilities
  *   run / run_with_outcomes       -> aleph_b200_apply_gate_stream
  *     (crates/aleph-backend/src/lib.rs:182-245)
@@ -284,6 +285,22 @@ int aleph_b200_sample_cumulative_noalloc(aleph_b200_handle* h, aleph_b200_state*
 /* ---- Backend::expectation_value (crates/aleph-sv/src/measure.rs:155-233) ---- */
 int aleph_b200_expectation(aleph_b200_handle* h, aleph_b200_state* st, const uint32_t* qubits,
                            const uint8_t* paulis, uint32_t n_terms, double coefficient, double* out);
+
+/* ---- expectation_pauli_sum (crates/aleph-backend/src/lib.rs:422-432) ----
+ * out = sum over terms k of coefficients[k] * Re <psi| P_k |psi>, where P_k is
+ * the Pauli string qubits[offsets[k] .. offsets[k+1]) with codes
+ * paulis[same range] (offsets has n_terms + 1 entries). The reference loops
+ * expectation_value over the terms; here the terms that share their X/Y
+ * positions are evaluated together, up to 16 per sweep of the state, and all
+ * results come back with one host synchronisation. Each term's value agrees
+ * with what aleph_b200_expectation returns for it to rounding (the same
+ * reduction order). Errors are the reference
+ * loop's: none for n_terms = 0; otherwise the state norm first, then each
+ * term's coefficient, qubit range and duplicates in term order.
+ * term_values (optional, n_terms doubles) receives each coefficients[k] * <P_k>. */
+int aleph_b200_expectation_sum(aleph_b200_handle* h, aleph_b200_state* st, const uint32_t* qubits,
+                               const uint8_t* paulis, const uint64_t* offsets, const double* coefficients,
+                               uint64_t n_terms, double* out, double* term_values);
 
 /* ---- Backend::probabilities (crates/aleph-sv/src/measure.rs:239-273): qubits[0] = LSB of the output index ---- */
 int aleph_b200_probabilities(aleph_b200_handle* h, aleph_b200_state* st, const uint32_t* qubits, uint32_t k,

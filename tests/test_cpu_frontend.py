@@ -197,3 +197,22 @@ def test_cli_errors_before_any_device_work(tmp_path, capsys):
     assert "references qubit 2 but circuit has 2 qubits" in capsys.readouterr().err
     assert cli_main(["run", str(ok), "--backend", "mps"]) == 1
     assert "unknown backend" in capsys.readouterr().err
+
+
+def test_maxcut_pauli_sum_terms():
+    """maxcut_pauli_sum (crates/aleph-ir/src/ansatz.rs:105-117): the identity
+    at |E|/2 first, then -1/2 Z_i Z_j per edge in edge order; an edge beyond
+    the register is an error."""
+    from aleph_b200 import workloads
+
+    assert workloads.maxcut_pauli_sum(2, [(0, 1)]) == [(0.5, []), (-0.5, [(0, "Z"), (1, "Z")])]
+    h = workloads.maxcut_pauli_sum(4, [(0, 1), (2, 3), (1, 3)])
+    assert h[0] == (1.5, []) and [t[1] for t in h[1:]] == [[(0, "Z"), (1, "Z")], [(2, "Z"), (3, "Z")],
+                                                              [(1, "Z"), (3, "Z")]]
+    # on a basis state the sum is the number of cut edges
+    x = 0b0101
+    cut = sum(((x >> i) & 1) != ((x >> j) & 1) for i, j in [(0, 1), (2, 3), (1, 3)])
+    val = sum(c * math.prod(-1 if (x >> q) & 1 else 1 for q, _ in s) for c, s in h)
+    assert val == cut
+    with pytest.raises(ValueError):
+        workloads.maxcut_pauli_sum(2, [(0, 2)])

@@ -230,6 +230,72 @@ def test_expectation_and_probabilities(n):
         assert np.abs(be.probabilities(st, sub) - oracle.probabilities(psi, sub)).max() <= 1e-12
 
 
+def random_pauli_sum(n, count, rng, flip_pool=3):
+    """Terms drawn so that several share their X/Y positions (more than 16
+    on the diagonal group), with identity and Y-carrying terms among them."""
+    flips = [[]] + [[int(q) for q in rng.permutation(n)[: int(rng.integers(1, 4))]] for _ in range(flip_pool)]
+    terms = []
+    for k in range(count):
+        xq = flips[int(rng.integers(0, len(flips)))] if k % 3 else []
+        rest = [int(q) for q in rng.permutation(n) if q not in xq][: int(rng.integers(0, 4))]
+        string = [(q, str(rng.choice(["X", "Y"]))) for q in xq] + [(q, str(rng.choice(["Z", "I"]))) for q in rest]
+        order = rng.permutation(len(string))
+        terms.append((float(rng.uniform(-2, 2)), [string[i] for i in order]))
+    return terms
+
+
+@pytest.mark.parametrize("n,precision", [(13, "f64"), (16, "f32")])
+def test_expectation_sum_matches_term_by_term(n, precision):
+    """aleph_b200_expectation_sum against the reference's loop over
+    expectation_value: each term's value agrees with the single-term result
+    to rounding (same reduction order; the compiler may contract the
+    per-amplitude products differently), the sum is taken in term order, and
+    it matches the oracle's."""
+    c = workloads.brickwall(n, 5, seed=40)
+    be = B200SvBackend(seed=0, precision=precision)
+    st = run(be, c)
+    psi = be.statevector(st)
+    rng = np.random.default_rng(41)
+    terms = random_pauli_sum(n, 45, rng)
+    total, vals = be.expectation_sum(st, terms, with_terms=True)
+    single = np.array([be.expectation_value(st, s, coef) for coef, s in terms])
+    assert np.abs(vals - single).max() <= 1e-13
+    assert total == sum(vals)  # summed in term order, as the reference does
+    ref = psi / np.linalg.norm(psi)  # the oracle holds a widened FP32 state to the FP64 norm tolerance
+    want = sum(oracle.expectation(ref, s, coef) for coef, s in terms)
+    assert abs(total - want) <= (1e-11 if precision == "f64" else 1e-5 * len(terms))
+    # Max-Cut: |E|/2 - 1/2 sum <Z_i Z_j>
+    edges = [(i, (i + 1) % n) for i in range(n)] + [(i, (i + 5) % n) for i in range(0, n, 2)]
+    h = workloads.maxcut_pauli_sum(n, edges)
+    assert be.expectation_sum(st, h) == pytest.approx(sum(be.expectation_value(st, s, coef) for coef, s in h),
+                                                      abs=1e-12)
+    be.close()
+
+
+def test_expectation_sum_errors():
+    """Errors in the reference loop's order: nothing for no terms; the state
+    first; then per term in order its coefficient, qubit range, duplicates."""
+    from aleph_b200 import backend as B
+
+    be = B200SvBackend(seed=0)
+    st = be.allocate(4)
+    assert be.expectation_sum(st, []) == 0.0
+    assert be.expectation_sum(st, [(0.75, [])]) == 0.75
+    with pytest.raises(B.DuplicateQubit):
+        be.expectation_sum(st, [(1.0, [(0, "Z")]), (1.0, [(1, "X"), (1, "Z")]), (1.0, [(9, "Z")])])
+    with pytest.raises(B.QubitOutOfRange):
+        be.expectation_sum(st, [(1.0, [(0, "Z")]), (1.0, [(9, "Z")]), (1.0, [(1, "X"), (1, "Z")])])
+    with pytest.raises(B.InvalidPauliString):
+        be.expectation_sum(st, [(1.0, [(0, "Z")]), (float("nan"), [(9, "Z")])])
+    bad = np.zeros(16, dtype=np.complex128)
+    bad[3] = 2.0
+    be.set_statevector(st, bad)
+    assert be.expectation_sum(st, []) == 0.0
+    with pytest.raises(B.InvalidState):
+        be.expectation_sum(st, [(float("nan"), [(9, "Z")])])
+    be.close()
+
+
 def test_norm_and_unpermute():
     n = 13
     c = workloads.brickwall(n, 4, seed=14)
