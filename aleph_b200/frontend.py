@@ -18,6 +18,7 @@ the reference's ChaCha12 stream).
 from __future__ import annotations
 
 import math
+import re
 import secrets
 from dataclasses import dataclass
 
@@ -147,6 +148,120 @@ def run(circuit, *, shots: int = DEFAULT_SHOTS, backend: str = "b200", precision
         raise
     label = f"seed={seed}" if seed is not None else "seed=entropy"
     return RunResult(be, state, counts_map(samples, circuit.num_qubits), outcomes, label)
+
+
+class PauliSumError(ValueError):
+    """``PauliSumError`` (crates/aleph-core/src/pauli.rs:89-108)."""
+
+
+# Rust's f64 grammar (what `str::parse::<f64>` accepts): optional sign, then
+# inf / infinity / nan in any case, or digits with an optional point and
+# exponent (".5" and "5." included; no underscores, no surrounding spaces)
+_RUST_F64 = re.compile(r"[+-]?(?:inf|infinity|nan|(?:\d+\.?\d*|\.\d+)(?:[eE][+-]?\d+)?)", re.IGNORECASE)
+
+
+def _rust_debug_str(s: str) -> str:
+    out = []
+    for ch in s:
+        if ch in ('"', "\\"):
+            out.append("\\" + ch)
+        elif ch == "\n":
+            out.append("\\n")
+        elif ch == "\r":
+            out.append("\\r")
+        elif ch == "\t":
+            out.append("\\t")
+        elif not ch.isprintable():
+            out.append(f"\\u{{{ord(ch):x}}}")
+        else:
+            out.append(ch)
+    return '"' + "".join(out) + '"'
+
+
+def _rust_debug_char(ch: str) -> str:
+    return "'" + ("\\'" if ch == "'" else _rust_debug_str(ch)[1:-1].replace('\\"', '"')) + "'"
+
+
+def _rust_lines(src: str):
+    """``str::lines``: split at \\n, drop one \\r before each \\n, no empty last line."""
+    parts = src.split("\n")
+    if parts and parts[-1] == "":
+        parts.pop()
+    for i, p in enumerate(parts):
+        if p.endswith("\r") and (i < len(parts) - 1 or src.endswith("\n")):
+            p = p[:-1]
+        yield p
+
+
+class PauliSum:
+    """``PauliSum`` (crates/aleph-core/src/pauli.rs:84-170): terms as
+    (coefficient, [(qubit, letter), ...]) with the qubits ascending and
+    identity factors dropped, as ``PauliString::new`` (pauli.rs:48-60) keeps them."""
+
+    def __init__(self, terms):
+        self.terms = list(terms)
+
+    @staticmethod
+    def parse(src: str, n_qubits: int) -> "PauliSum":
+        """One term per line, ``<coeff> <pauli>``; character i of ``<pauli>``
+        is the Pauli on qubit i; blank lines and ``#`` lines are skipped."""
+        terms = []
+        for idx, raw in enumerate(_rust_lines(src)):
+            line = idx + 1
+            trimmed = raw.strip()
+            if not trimmed or trimmed.startswith("#"):
+                continue
+            parts = trimmed.split()
+            if len(parts) != 2:
+                raise PauliSumError(f"line {line}: expected '<coeff> <pauli>', got {_rust_debug_str(raw)}")
+            coeff_s, pauli_s = parts
+            if not _RUST_F64.fullmatch(coeff_s):
+                raise PauliSumError(f"line {line}: coefficient {_rust_debug_str(coeff_s)} is not a finite float")
+            coeff = float(coeff_s)
+            if len(pauli_s) != n_qubits:
+                raise PauliSumError(f"line {line}: pauli string has {len(pauli_s)} chars, expected {n_qubits}")
+            factors = []
+            for q, ch in enumerate(pauli_s):
+                if ch not in "IXYZ":
+                    raise PauliSumError(f"line {line}: {_rust_debug_char(ch)} is not one of I,X,Y,Z")
+                if ch != "I":
+                    factors.append((q, ch))
+            if not math.isfinite(coeff):
+                raise PauliSumError(f"line {line}: non-finite coefficient")
+            terms.append((coeff, factors))
+        return PauliSum(terms)
+
+    @staticmethod
+    def load(path: str, n_qubits: int) -> "PauliSum":
+        """``PauliSum.load`` (crates/aleph-py/src/energy.rs:24-31)."""
+        try:
+            with open(path, encoding="utf-8") as f:
+                src = f.read()
+        except OSError as e:
+            raise ValueError(f"read {path}: {e}") from e
+        try:
+            return PauliSum.parse(src, n_qubits)
+        except PauliSumError as e:
+            raise ValueError(f"parse {path}: {e}") from e
+
+    def num_terms(self) -> int:
+        return len(self.terms)
+
+
+def hea_energy(n_qubits: int, depth: int, thetas, ham: PauliSum, backend: str = "b200",
+               precision: str = "f64") -> float:
+    """⟨ψ(θ)|H|ψ(θ)⟩ of the Ry + CNOT hardware-efficient ansatz (``hea_energy``,
+    crates/aleph-py/src/energy.rs:40-55): ``build_hea`` then one fused
+    Pauli-sum expectation of ``ham``."""
+    from . import workloads
+
+    circuit = workloads.build_hea(n_qubits, depth, list(thetas))
+    be = B200SvBackend(seed=0, precision=resolve(backend, precision))
+    try:
+        state, _ = run_with_outcomes(be, circuit)
+        return float(be.expectation_sum(state, ham.terms))
+    finally:
+        be.close()
 
 
 def qaoa_energy(n_qubits: int, edges, gammas, betas, backend: str = "b200", precision: str = "f64") -> float:

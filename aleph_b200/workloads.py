@@ -153,6 +153,24 @@ def grover(n_data: int, marked: int, iterations: int) -> C.Circuit:
     return c
 
 
+def build_hea(n: int, depth: int, params) -> C.Circuit:
+    """``build_hea`` (crates/aleph-ir/src/ansatz.rs:32-61): ``depth`` layers of
+    Ry on every qubit followed by the CNOT chain (q, q+1), then a final Ry
+    layer; ``params[layer * n + q]`` drives qubit q in rotation layer
+    ``layer`` (0..=depth)."""
+    expected = n * (depth + 1)
+    if len(params) != expected:
+        raise ValueError(f"expected {expected} params (n_qubits*(depth+1)), got {len(params)}")
+    c = C.Circuit(n)
+    for layer in range(depth + 1):
+        for q in range(n):
+            c.add(C.Ry(float(params[layer * n + q])), [q])
+        if layer < depth:
+            for q in range(n - 1):
+                c.add(C.Cnot(), [q, q + 1])
+    return c
+
+
 def maxcut_pauli_sum(n: int, edges):
     """``maxcut_pauli_sum`` (crates/aleph-ir/src/ansatz.rs:105-117): the
     identity with coefficient |E|/2, then -1/2 Z_i Z_j per edge, as

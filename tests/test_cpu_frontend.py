@@ -216,3 +216,55 @@ def test_maxcut_pauli_sum_terms():
     assert val == cut
     with pytest.raises(ValueError):
         workloads.maxcut_pauli_sum(2, [(0, 2)])
+
+
+def test_pauli_sum_text_format():
+    """PauliSum::parse (crates/aleph-core/src/pauli.rs:115-170): comments,
+    blanks, trailing identities dropped, the identity term, every error."""
+    h = frontend.PauliSum.parse("# H2-like\n\n0.5 ZI\n  0.25 XX  \n-1.5 II\n", 2)
+    assert h.num_terms() == 3
+    assert h.terms == [(0.5, [(0, "Z")]), (0.25, [(0, "X"), (1, "X")]), (-1.5, [])]
+    assert frontend.PauliSum.parse("1e-3 YZ\r\n", 2).terms == [(1e-3, [(0, "Y"), (1, "Z")])]
+    bad = {
+        "0.5\n": "line 1: expected '<coeff> <pauli>', got \"0.5\"",
+        "\n0.5 ZZ X\n": "line 2: expected '<coeff> <pauli>', got \"0.5 ZZ X\"",
+        "half ZZ\n": "line 1: coefficient \"half\" is not a finite float",
+        "1_0 ZZ\n": "line 1: coefficient \"1_0\" is not a finite float",
+        "0.5 ZZZ\n": "line 1: pauli string has 3 chars, expected 2",
+        "0.5 ZA\n": "line 1: 'A' is not one of I,X,Y,Z",
+        "inf ZZ\n": "line 1: non-finite coefficient",
+    }
+    for src, msg in bad.items():
+        with pytest.raises(frontend.PauliSumError) as e:
+            frontend.PauliSum.parse(src, 2)
+        assert str(e.value) == msg
+
+
+def test_pauli_sum_load(tmp_path):
+    p = tmp_path / "h.txt"
+    p.write_text("0.5 ZZ\n0.5 XQ\n")
+    with pytest.raises(ValueError, match=r"^parse .*h\.txt: line 2: 'Q' is not one of I,X,Y,Z$"):
+        frontend.PauliSum.load(str(p), 2)
+    with pytest.raises(ValueError, match=r"^read .*missing\.txt: "):
+        frontend.PauliSum.load(str(tmp_path / "missing.txt"), 2)
+    p.write_text("0.5 ZZ\n-0.25 XY\n")
+    assert frontend.PauliSum.load(str(p), 2).terms == [(0.5, [(0, "Z"), (1, "Z")]), (-0.25, [(0, "X"), (1, "Y")])]
+
+
+def test_build_hea_layout():
+    """build_hea (crates/aleph-ir/src/ansatz.rs:32-61): Ry layer + CNOT chain
+    per entangling layer, a final Ry layer; params[layer * n + q]."""
+    from aleph_b200 import workloads
+
+    n, depth = 3, 2
+    params = [0.1 * (i + 1) for i in range(n * (depth + 1))]
+    c = workloads.build_hea(n, depth, params)
+    got = [(g.gate.name, list(g.qubits), g.gate.params) for g in c.instructions]
+    want = []
+    for layer in range(depth + 1):
+        want += [("Ry", [q], (params[layer * n + q],)) for q in range(n)]
+        if layer < depth:
+            want += [("Cnot", [q, q + 1], ()) for q in range(n - 1)]
+    assert got == want
+    with pytest.raises(ValueError, match=r"expected 9 params \(n_qubits\*\(depth\+1\)\), got 8"):
+        workloads.build_hea(n, depth, params[:-1])

@@ -124,3 +124,39 @@ def test_qaoa_energy_against_the_oracle():
     got = frontend.qaoa_energies([(n, edges)], [g], [b], sweep_max_n=0)[0]
     assert got == pytest.approx(want, abs=1e-9)
     assert frontend.qaoa_energy(n, edges, g, b, precision="f32") == pytest.approx(want, rel=2e-5)
+
+
+def _synthetic_hamiltonian(n, count, seed):
+    """A seeded stand-in for a VQE Hamiltonian in the committed text format."""
+    rng = np.random.default_rng(seed)
+    lines = ["# synthetic: seeded Pauli terms"]
+    for _ in range(count):
+        lines.append(f"{rng.uniform(-1, 1):.12f} " + "".join(rng.choice(list("IIXYZ"), size=n)))
+    return "\n".join(lines) + "\n"
+
+
+def test_hea_energy_against_the_oracle():
+    n, depth = 6, 3
+    ham = frontend.PauliSum.parse(_synthetic_hamiltonian(n, 40, 11), n)
+    rng = np.random.default_rng(12)
+    thetas = rng.uniform(-np.pi, np.pi, n * (depth + 1))
+    psi, _ = oracle.run(n, workloads.build_hea(n, depth, thetas).instructions)
+    want = sum(oracle.expectation(psi, s, c) for c, s in ham.terms)
+    assert frontend.hea_energy(n, depth, thetas, ham) == pytest.approx(want, abs=1e-12)
+    assert frontend.hea_energy(n, depth, thetas, ham, precision="f32") == pytest.approx(want, abs=5e-5)
+    assert frontend.hea_energy(n, depth, thetas, ham, precision="tc32") == pytest.approx(want, abs=5e-5)
+
+
+def test_hea_energy_is_sinusoidal_in_each_angle():
+    """Each Ry angle enters as exp(-i theta Y / 2): E(theta_j) = A cos(theta_j - phi) + c,
+    so E(b) + E(b + pi) = E(b + pi/2) + E(b - pi/2) (the identity rotosolve
+    steps on, benches/tests/vqe_h2_convergence.rs)."""
+    n, depth = 5, 2
+    ham = frontend.PauliSum.parse(_synthetic_hamiltonian(n, 25, 13), n)
+    base = [0.1 * (i + 1) for i in range(n * (depth + 1))]
+    for j in (0, 7, len(base) - 1):
+        def e(shift):
+            t = list(base)
+            t[j] += shift
+            return frontend.hea_energy(n, depth, t, ham)
+        assert e(0.0) + e(np.pi) == pytest.approx(e(np.pi / 2) + e(-np.pi / 2), abs=1e-12)
