@@ -129,6 +129,20 @@ class Stats(ct.Structure):
     ]
 
 
+class PagedInfo(ct.Structure):
+    _fields_ = [
+        ("num_qubits", ct.c_uint32),
+        ("tile_qubits", ct.c_uint32),
+        ("local_qubits", ct.c_uint32),
+        ("depth", ct.c_uint32),
+        ("segments", ct.c_uint64),
+        ("groups", ct.c_uint64),
+        ("h2d_bytes", ct.c_uint64),
+        ("d2h_bytes", ct.c_uint64),
+        ("seconds", ct.c_double),
+    ]
+
+
 class PassRecord(ct.Structure):
     _fields_ = [
         ("kind", ct.c_uint32),
@@ -225,6 +239,13 @@ _SIGNATURES = {
     "aleph_b200_get_pass_records": ([_P, ct.POINTER(PassRecord), ct.c_uint64, ct.POINTER(ct.c_uint64)], ct.c_int),
     "aleph_b200_get_stats": ([_P, ct.POINTER(Stats)], ct.c_int),
     "aleph_b200_reset_stats": ([_P], ct.c_int),
+    "aleph_b200_paged_run": (
+        [_P, ct.c_uint32, ct.POINTER(Instr), ct.c_uint64, ct.POINTER(Pools), ct.c_uint32, ct.c_uint32,
+         ct.POINTER(_P)], ct.c_int),
+    "aleph_b200_paged_info_get": ([_P, ct.POINTER(PagedInfo)], ct.c_int),
+    "aleph_b200_paged_get_amplitudes": ([_P, ct.POINTER(ct.c_double)], ct.c_int),
+    "aleph_b200_paged_norm_sqr": ([_P, ct.POINTER(ct.c_double)], ct.c_int),
+    "aleph_b200_paged_free": ([_P], ct.c_int),
 }
 
 _LIB = None

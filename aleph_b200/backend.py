@@ -70,6 +70,40 @@ class State:
         return self.backend.statevector(self)
 
 
+class PagedState:
+    """An out-of-core state: the amplitudes live in pinned host memory
+    (``PagedSvState``, crates/aleph-cuda/src/sv/paged.rs:53-100)."""
+
+    def __init__(self, lib, ptr, num_qubits: int):
+        self.lib, self.ptr, self.num_qubits = lib, ptr, num_qubits
+
+    def statevector(self) -> np.ndarray:
+        out = np.empty(2 << self.num_qubits, dtype=np.float64)
+        self.lib.aleph_b200_paged_get_amplitudes(self.ptr, out.ctypes.data_as(ct.POINTER(ct.c_double)))
+        return out.view(np.complex128)
+
+    def norm_sqr(self) -> float:
+        v = ct.c_double()
+        self.lib.aleph_b200_paged_norm_sqr(self.ptr, ct.byref(v))
+        return v.value
+
+    def info(self) -> dict:
+        i = abi.PagedInfo()
+        self.lib.aleph_b200_paged_info_get(self.ptr, ct.byref(i))
+        return {name: getattr(i, name) for name, _ in abi.PagedInfo._fields_}
+
+    def free(self):
+        if self.ptr:
+            self.lib.aleph_b200_paged_free(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
 @dataclass
 class MeasurementRecord:
     """``MeasurementRecord`` (crates/aleph-backend/src/lib.rs:188-195)."""
@@ -270,6 +304,17 @@ class B200SvBackend:
             u.ctypes.data_as(ct.POINTER(ct.c_double)) if u is not None and u.size else None,
             0 if u is None else u.size, outs, flat.n, ct.byref(nout)))
         return [int(outs[i]) for i in range(nout.value)]
+
+    def run_paged(self, circuit: Circuit, tile_qubits: int, depth: int = 3) -> PagedState:
+        """``CudaSvBackend::run_paged`` / ``run_paged_overlapped``
+        (crates/aleph-cuda/src/sv/paged.rs:138-276): run ``circuit`` with the
+        state in pinned host memory, 2^tile_qubits-amplitude tiles streamed
+        through the device (``depth`` device buffers; 1 = no copy overlap)."""
+        flat = flatten(circuit.instructions)
+        out = ct.c_void_p()
+        self._check(self.lib.aleph_b200_paged_run(self.handle, circuit.num_qubits, flat.instrs, flat.n,
+                                                  ct.byref(flat.pools), int(tile_qubits), int(depth), ct.byref(out)))
+        return PagedState(self.lib, out, circuit.num_qubits)
 
     def qaoa_sweep(self, graphs, gammas, betas) -> np.ndarray:
         """<C> of the build_qaoa Max-Cut circuit (crates/aleph-ir/src/ansatz.rs:71-117)

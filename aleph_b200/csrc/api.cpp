@@ -7,6 +7,7 @@
 // in the CUDA kernels of this library.
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -113,6 +114,12 @@ int cuda_fail(aleph_b200_handle* h, cudaError_t err, const char* what) {
   do {                                                   \
     cudaError_t _e = (expr);                             \
     if (_e != cudaSuccess) return cuda_fail(h, _e, what); \
+  } while (0)
+// CK that first runs a cleanup callable on the status it returns
+#define CK_OR(expr, cleanup, what)                                 \
+  do {                                                             \
+    cudaError_t _e = (expr);                                       \
+    if (_e != cudaSuccess) return cleanup(cuda_fail(h, _e, what)); \
   } while (0)
 
 int ensure(aleph_b200_handle* h, Scratch& s, size_t bytes) {
@@ -323,7 +330,7 @@ int execute(aleph_b200_handle* h, aleph_b200_state* st, const Plan& P, const dou
   }
   bool any_block = false;
   for (const Pass& ps : P.passes) any_block |= ps.kind == PASS_BLOCK;
-  if (any_block) {
+  if (any_block && P.renormalize) {
     if (int r = ensure(h, h->reduce, (size_t)nb * 3 * 8 + 256)) return r;
     double* part = (double*)h->reduce.ptr;
     CK(record_begin(pk), "event record");
@@ -751,6 +758,339 @@ int aleph_b200_plan_free(aleph_b200_handle* h, aleph_b200_plan* plan) {
     cudaFree(plan->buf.ptr);
   }
   delete plan;
+  return ALEPH_B200_OK;
+}
+
+// ---- out-of-core runs --------------------------------------------------------
+// crates/aleph-cuda/src/sv/paged.rs:1-38 (tiling scheme), :138-251
+// (run_paged), :253-276 (run_paged_overlapped). The reference gathers the
+// tiles of one gate at a time; here a segment of gates shares one gather, so
+// the host state is read and written once per segment, not once per gate.
+struct aleph_b200_paged_state {
+  uint32_t n = 0;
+  int precision = ALEPH_B200_F64;
+  void* host = nullptr;  // pinned, 2^n amplitudes
+  size_t bytes = 0;
+  aleph_b200_paged_info info{};
+};
+
+namespace {
+
+uint64_t deposit_bits(uint64_t v, const std::vector<uint32_t>& positions) {  // bit i of v -> bit positions[i]
+  uint64_t r = 0;
+  for (size_t i = 0; i < positions.size(); ++i) r |= ((v >> i) & 1) << positions[i];
+  return r;
+}
+
+uint64_t qubit_mask(const aleph_b200_instr& r, uint32_t n) {  // targets and controls
+  uint64_t mask = 0;
+  for (uint32_t k = 0; k < r.num_qubits && k < 8; ++k)
+    if (r.qubits[k] < n) mask |= 1ull << r.qubits[k];
+  for (uint32_t k = 0; k < r.num_controls && k < 8; ++k)
+    if (r.controls[k] < n) mask |= 1ull << r.controls[k];
+  return mask;
+}
+uint64_t high_mask(const aleph_b200_instr& r, uint32_t m, uint32_t n) {
+  return qubit_mask(r, n) & ~((1ull << m) - 1);
+}
+
+struct PagedRing {
+  int device = 0;
+  std::vector<void*> buf;
+  std::vector<cudaEvent_t> in, done, out;
+  cudaStream_t h2d = nullptr, d2h = nullptr;
+  ~PagedRing() {
+    cudaSetDevice(device);
+    if (h2d) cudaStreamSynchronize(h2d);
+    if (d2h) cudaStreamSynchronize(d2h);
+    for (void* p : buf) cudaFree(p);
+    for (auto* v : {&in, &done, &out})
+      for (cudaEvent_t e : *v) cudaEventDestroy(e);
+    if (h2d) cudaStreamDestroy(h2d);
+    if (d2h) cudaStreamDestroy(d2h);
+  }
+};
+
+}  // namespace
+
+int aleph_b200_paged_run(aleph_b200_handle* h, uint32_t n, const aleph_b200_instr* in, uint64_t count,
+                         const aleph_b200_pools* pools, uint32_t m, uint32_t depth, aleph_b200_paged_state** out) {
+  if (!h || !out || (!in && count)) return ALEPH_B200_INVALID_ARGUMENT;
+  *out = nullptr;
+  if (n == 0 && count == 0) {
+    aleph_b200_error_info e{};
+    e.status = ALEPH_B200_EMPTY_CIRCUIT;
+    return report(h, e);
+  }
+  if (m == 0 || m >= n) {
+    aleph_b200_error_info e{};
+    e.status = ALEPH_B200_INVALID_STATE;
+    std::snprintf(e.kind, sizeof(e.kind), "paged tile_qubits must satisfy 1 <= tile_qubits < num_qubits");
+    return report(h, e);
+  }
+  if (n > kMaxQubits) {
+    aleph_b200_error_info e{};
+    e.status = ALEPH_B200_TOO_MANY_QUBITS;
+    e.requested = n;
+    e.limit = kMaxQubits;
+    return report(h, e);
+  }
+  if (depth == 0) depth = 3;
+  if (depth > 8) depth = 8;
+  // one scan (paged.rs:161-185): unsupported instructions, the widest gate
+  uint32_t g_max = 0;
+  for (uint64_t i = 0; i < count; ++i) {
+    const char* kind = nullptr;
+    switch (in[i].kind) {
+      case ALEPH_INSTR_MEASURE: kind = "measure"; break;
+      case ALEPH_INSTR_RESET: kind = "reset"; break;
+      case ALEPH_INSTR_DIAGONAL_PHASE: kind = "diagonal-phase"; break;
+      case ALEPH_INSTR_TILED_BLOCK: kind = "tiled-block"; break;
+      case ALEPH_INSTR_BARRIER: continue;
+      default: break;
+    }
+    if (kind) {
+      aleph_b200_error_info e{};
+      e.status = ALEPH_B200_UNSUPPORTED_INSTRUCTION;
+      e.instruction = i;
+      std::snprintf(e.kind, sizeof(e.kind), "%s", kind);
+      return report(h, e);
+    }
+    g_max = std::max<uint32_t>(g_max, (uint32_t)__builtin_popcountll(high_mask(in[i], m, n)));
+  }
+  if (int r = bind(h)) return r;
+  const int prec = h->precision == ALEPH_B200_F64 ? ALEPH_B200_F64 : ALEPH_B200_F32;
+  const size_t bpa = prec == ALEPH_B200_F64 ? 16 : 8;
+  // the largest tile group the device holds: `depth` buffers in half of the free memory
+  size_t free_b = 0, total_b = 0;
+  CK(cudaMemGetInfo(&free_b, &total_b), "memory info");
+  uint32_t L = std::min<uint32_t>(n, std::min<uint32_t>(h->qubit_cap, kMaxQubits));
+  if (h->paged_local_max) L = std::min<uint32_t>(L, std::max<uint32_t>(h->paged_local_max, m));
+  while (L > m && (double)depth * (double)(bpa << L) > 0.5 * (double)free_b) --L;
+  if (m + g_max > L || (double)depth * (double)(bpa << m) > 0.5 * (double)free_b) {
+    aleph_b200_error_info e{};
+    e.status = ALEPH_B200_TOO_MANY_QUBITS;
+    e.requested = m + g_max;
+    e.limit = L;
+    return report(h, e);
+  }
+  const uint32_t g_budget = L - m;
+  // every gate validated against the full register first (same checks and
+  // payloads as the in-core stream); nothing is allocated before this passes
+  {
+    std::vector<Lowered> ops;
+    if (int r = lower_stream(h, n, in, count, pools, &ops)) return r;
+  }
+  // segments: each takes, in order, every remaining gate whose high qubits
+  // fit the budget and that shares no qubit with a gate it leaves for later
+  // (so it commutes with all of them: the reordering is exact)
+  struct Segment {
+    std::vector<uint64_t> gates;
+    uint64_t hmask;
+  };
+  std::vector<Segment> segs;
+  {
+    std::vector<uint64_t> remaining, deferred;
+    for (uint64_t i = 0; i < count; ++i)
+      if (in[i].kind != ALEPH_INSTR_BARRIER) remaining.push_back(i);
+    while (!remaining.empty()) {
+      Segment sg{{}, 0};
+      uint64_t blocked = 0;
+      deferred.clear();
+      for (uint64_t i : remaining) {
+        const uint64_t qm = qubit_mask(in[i], n), gm = qm & ~((1ull << m) - 1);
+        if (!(qm & blocked) && (uint32_t)__builtin_popcountll(sg.hmask | gm) <= g_budget) {
+          sg.gates.push_back(i);
+          sg.hmask |= gm;
+        } else {
+          deferred.push_back(i);
+          blocked |= qm;
+        }
+      }
+      segs.push_back(std::move(sg));
+      remaining.swap(deferred);
+    }
+  }
+  uint32_t l_used = m;
+  for (const Segment& sg : segs) l_used = std::max<uint32_t>(l_used, m + (uint32_t)__builtin_popcountll(sg.hmask));
+
+  aleph_b200_paged_state* ps = new (std::nothrow) aleph_b200_paged_state();
+  if (!ps) return set_error(h, ALEPH_B200_DEVICE_FAILURE, "host allocation failed");
+  ps->n = n;
+  ps->precision = prec;
+  ps->bytes = bpa << n;
+  cudaError_t ce = cudaHostAlloc(&ps->host, ps->bytes, cudaHostAllocPortable);
+  if (ce != cudaSuccess) {
+    cudaGetLastError();
+    delete ps;
+    return cuda_fail(h, ce, "pinned host state allocation");
+  }
+  std::memset(ps->host, 0, ps->bytes);
+  if (prec == ALEPH_B200_F64) ((double*)ps->host)[0] = 1.0;
+  else ((float*)ps->host)[0] = 1.0f;
+  auto fail = [&](int r) {
+    aleph_b200_paged_free(ps);
+    return r;
+  };
+  const auto t0 = std::chrono::steady_clock::now();
+
+  PagedRing ring;
+  ring.device = h->device;
+  const size_t buf_bytes = bpa << l_used;
+  ring.buf.assign(depth, nullptr);
+  ring.in.assign(depth, nullptr);
+  ring.done.assign(depth, nullptr);
+  ring.out.assign(depth, nullptr);
+  for (uint32_t k = 0; k < depth; ++k) {
+    if ((ce = cudaMalloc(&ring.buf[k], buf_bytes)) != cudaSuccess ||
+        (ce = cudaEventCreateWithFlags(&ring.in[k], cudaEventDisableTiming)) != cudaSuccess ||
+        (ce = cudaEventCreateWithFlags(&ring.done[k], cudaEventDisableTiming)) != cudaSuccess ||
+        (ce = cudaEventCreateWithFlags(&ring.out[k], cudaEventDisableTiming)) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(cuda_fail(h, ce, "paged device ring"));
+    }
+  }
+  if ((ce = cudaStreamCreateWithFlags(&ring.h2d, cudaStreamNonBlocking)) != cudaSuccess ||
+      (ce = cudaStreamCreateWithFlags(&ring.d2h, cudaStreamNonBlocking)) != cudaSuccess)
+    return fail(cuda_fail(h, ce, "paged copy streams"));
+
+  const size_t tile_bytes = bpa << m;
+  uint64_t group = 0;  // global group counter: ring slot = group % depth
+  aleph_b200_paged_info& info = ps->info;
+  info.num_qubits = n;
+  info.tile_qubits = m;
+  info.local_qubits = l_used;
+  info.depth = depth;
+  std::vector<aleph_b200_instr> local;
+  for (size_t si = 0; si < segs.size(); ++si) {
+    const Segment& sg = segs[si];
+    std::vector<uint32_t> H, R;  // the segment's high qubits / the other high qubits, ascending
+    for (uint32_t q = m; q < n; ++q) ((sg.hmask >> q) & 1 ? H : R).push_back(q);
+    const uint32_t hh = (uint32_t)H.size(), nl = m + hh;
+    std::vector<uint32_t> to_local(n);
+    for (uint32_t q = 0; q < m; ++q) to_local[q] = q;
+    for (uint32_t r = 0; r < hh; ++r) to_local[H[r]] = m + r;
+    // the segment on its local register, compiled once
+    local.clear();
+    for (uint64_t i : sg.gates) local.push_back(in[i]);
+    for (aleph_b200_instr& r : local) {
+      for (uint32_t k = 0; k < r.num_qubits && k < 8; ++k) r.qubits[k] = to_local[r.qubits[k]];
+      for (uint32_t k = 0; k < r.num_controls && k < 8; ++k) r.controls[k] = to_local[r.controls[k]];
+    }
+    Plan P;
+    {
+      std::vector<Lowered> ops;
+      if (int r = lower_stream(h, nl, local.data(), local.size(), pools, &ops)) return fail(r);
+      if (int s = build_plan(ops, nl, h->opts, &P)) return fail(set_error(h, s, "optimization pipeline failed: planner"));
+      P.renormalize = false;
+    }
+    Scratch plan_buf;
+    bool uploaded = false;
+    // tile index bit (q - m) <-> qubit q
+    std::vector<uint32_t> hbit(hh), rbit(R.size());
+    for (uint32_t r = 0; r < hh; ++r) hbit[r] = H[r] - m;
+    for (size_t r = 0; r < R.size(); ++r) rbit[r] = R[r] - m;
+    const uint64_t n_outer = 1ull << R.size(), n_sub = 1ull << hh;
+    auto copies = [&](uint64_t outer, uint32_t slot, bool to_device) -> cudaError_t {
+      const uint64_t base = deposit_bits(outer, rbit);
+      for (uint64_t s = 0; s < n_sub; ++s) {
+        const uint64_t tile = base | deposit_bits(s, hbit);
+        char* hp = (char*)ps->host + tile * tile_bytes;
+        char* dp = (char*)ring.buf[slot] + s * tile_bytes;
+        const cudaError_t e = to_device
+                                  ? cudaMemcpyAsync(dp, hp, tile_bytes, cudaMemcpyHostToDevice, ring.h2d)
+                                  : cudaMemcpyAsync(hp, dp, tile_bytes, cudaMemcpyDeviceToHost, ring.d2h);
+        if (e != cudaSuccess) return e;
+      }
+      (to_device ? info.h2d_bytes : info.d2h_bytes) += n_sub * tile_bytes;
+      return cudaSuccess;
+    };
+    // gather of group g (outer index o): waits for the slot's previous scatter
+    // and, for a segment's first group, for every scatter of the segment
+    // before (the tiles it reads were written there; d2h is in order)
+    auto gather = [&](uint64_t g, uint64_t o, bool first_of_segment) -> cudaError_t {
+      const uint32_t slot = (uint32_t)(g % depth);
+      cudaError_t e = cudaSuccess;
+      if (g >= depth) e = cudaStreamWaitEvent(ring.h2d, ring.out[slot], 0);
+      if (e == cudaSuccess && first_of_segment && g > 0)
+        e = cudaStreamWaitEvent(ring.h2d, ring.out[(g - 1) % depth], 0);
+      if (e == cudaSuccess) e = copies(o, slot, true);
+      if (e == cudaSuccess) e = cudaEventRecord(ring.in[slot], ring.h2d);
+      return e;
+    };
+    const uint64_t g0 = group;
+    CK_OR(gather(g0, 0, true), fail, "paged gather");
+    for (uint64_t o = 0; o < n_outer; ++o) {
+      const uint64_t g = g0 + o;
+      const uint32_t slot = (uint32_t)(g % depth);
+      // the next group's gather runs while this one computes (another slot)
+      if (depth > 1 && o + 1 < n_outer) CK_OR(gather(g + 1, o + 1, false), fail, "paged gather");
+      CK_OR(cudaStreamWaitEvent(h->stream, ring.in[slot], 0), fail, "stream wait");
+      aleph_b200_state st;
+      st.n = nl;
+      st.precision = prec;
+      st.amps = ring.buf[slot];
+      st.bytes = bpa << nl;
+      if (int r = run_plan(h, &st, P, nullptr, 0, nullptr, 0, nullptr, nullptr, &plan_buf, &uploaded)) {
+        if (plan_buf.ptr) cudaFree(plan_buf.ptr);
+        return fail(r);
+      }
+      CK_OR(cudaEventRecord(ring.done[slot], h->stream), fail, "event record");
+      CK_OR(cudaStreamWaitEvent(ring.d2h, ring.done[slot], 0), fail, "stream wait");
+      CK_OR(copies(o, slot, false), fail, "paged scatter");
+      CK_OR(cudaEventRecord(ring.out[slot], ring.d2h), fail, "event record");
+      if (depth == 1 && o + 1 < n_outer) CK_OR(gather(g + 1, o + 1, false), fail, "paged gather");
+    }
+    group += n_outer;
+    info.groups += n_outer;
+    ++info.segments;
+    cudaStreamSynchronize(h->stream);
+    if (plan_buf.ptr) cudaFree(plan_buf.ptr);
+  }
+  CK_OR(cudaStreamSynchronize(ring.d2h), fail, "stream synchronize");
+  CK_OR(cudaStreamSynchronize(ring.h2d), fail, "stream synchronize");
+  info.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  *out = ps;
+  return ALEPH_B200_OK;
+}
+
+int aleph_b200_paged_info_get(const aleph_b200_paged_state* ps, aleph_b200_paged_info* out) {
+  if (!ps || !out) return ALEPH_B200_INVALID_ARGUMENT;
+  *out = ps->info;
+  return ALEPH_B200_OK;
+}
+
+int aleph_b200_paged_get_amplitudes(const aleph_b200_paged_state* ps, double* out) {
+  if (!ps || !out) return ALEPH_B200_INVALID_ARGUMENT;
+  const uint64_t len = 1ull << ps->n;
+  if (ps->precision == ALEPH_B200_F64) {
+    std::memcpy(out, ps->host, ps->bytes);
+  } else {
+    const float* f = (const float*)ps->host;
+    for (uint64_t i = 0; i < 2 * len; ++i) out[i] = f[i];
+  }
+  return ALEPH_B200_OK;
+}
+
+int aleph_b200_paged_norm_sqr(const aleph_b200_paged_state* ps, double* out) {
+  if (!ps || !out) return ALEPH_B200_INVALID_ARGUMENT;
+  const uint64_t len = 1ull << ps->n;
+  double s = 0.0;
+  if (ps->precision == ALEPH_B200_F64) {
+    const double* d = (const double*)ps->host;
+    for (uint64_t i = 0; i < 2 * len; ++i) s += d[i] * d[i];
+  } else {
+    const float* f = (const float*)ps->host;
+    for (uint64_t i = 0; i < 2 * len; ++i) s += (double)f[i] * (double)f[i];
+  }
+  *out = s;
+  return ALEPH_B200_OK;
+}
+
+int aleph_b200_paged_free(aleph_b200_paged_state* ps) {
+  if (!ps) return ALEPH_B200_OK;
+  if (ps->host) cudaFreeHost(ps->host);
+  delete ps;
   return ALEPH_B200_OK;
 }
 
@@ -1427,6 +1767,12 @@ int aleph_b200_set_tuning(aleph_b200_handle* h, const char* key, int64_t value) 
   }
   if (!std::strcmp(key, "relabel_swaps")) {
     h->opts.relabel_swaps = value != 0;
+    return ALEPH_B200_OK;
+  }
+  if (!std::strcmp(key, "paged_local_qubits")) {
+    if (value < 0 || value > (int64_t)kMaxQubits)
+      return set_error(h, ALEPH_B200_INVALID_ARGUMENT, "paged_local_qubits must be in 0..%u", kMaxQubits);
+    h->paged_local_max = (uint32_t)value;
     return ALEPH_B200_OK;
   }
   return set_error(h, ALEPH_B200_INVALID_ARGUMENT, "unknown tuning key %s", key);

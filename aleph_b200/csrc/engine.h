@@ -136,6 +136,9 @@ struct Plan {
   // TC32 split-BF16 block operand images (bytes), one 64 KiB image per block
   std::vector<uint8_t> block_images;
   uint32_t n_measures = 0;
+  // TC32: renormalise the state after the block passes. Off for plans that
+  // run on one tile group of an out-of-core state, whose norm is not 1.
+  bool renormalize = true;
 };
 
 struct PlanOptions {
@@ -174,6 +177,9 @@ struct Handle {
   aleph_b200_stats stats{};
   PlanOptions opts;
   int sm_count = 148;
+  // out-of-core runs: cap on the qubits of one device tile group (0: the
+  // most that `depth` buffers fit in half of the free device memory)
+  uint32_t paged_local_max = 0;
   // device scratch (grown on demand, freed with the handle)
   Scratch reduce;    // reduction partials
   Scratch plan_buf;  // uploaded plan tables

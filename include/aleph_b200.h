@@ -17,6 +17,8 @@
  *   Backend::probabilities        -> aleph_b200_probabilities
  *   run / run_with_outcomes       -> aleph_b200_apply_gate_stream
  *     (crates/aleph-backend/src/lib.rs:182-245)
+ *   CudaSvBackend::run_paged[_overlapped] -> aleph_b200_paged_run
+ *     (crates/aleph-cuda/src/sv/paged.rs:138-276)
  *
  * Every function returns an aleph_b200_status (0 = OK). Non-zero codes map
  * 1:1 onto the variants of `BackendError` (crates/aleph-backend/src/lib.rs:22-74);
@@ -328,7 +330,9 @@ int aleph_b200_last_error_info(const aleph_b200_handle* h, aleph_b200_error_info
  * (0/1: time every pass of later gate streams with CUDA events),
  * "relabel_swaps" (0/1, default 1: an uncontrolled SWAP of a state larger
  * than smem_max_n relabels qubits instead of moving data, and one or two
- * in-place permutation passes settle the labels at the end of the stream). */
+ * in-place permutation passes settle the labels at the end of the stream),
+ * "paged_local_qubits" (0..40, default 0: the most qubits one device tile
+ * group of an out-of-core run may hold; 0 lets free device memory decide). */
 int aleph_b200_set_tuning(aleph_b200_handle* h, const char* key, int64_t value);
 
 /* ---- per-pass timing records (training data of the learned fusion planner) ---- */
@@ -402,6 +406,43 @@ typedef struct aleph_b200_stats {
 } aleph_b200_stats;
 int aleph_b200_get_stats(const aleph_b200_handle* h, aleph_b200_stats* out);
 int aleph_b200_reset_stats(aleph_b200_handle* h);
+
+/* ---- out-of-core runs (crates/aleph-cuda/src/sv/paged.rs:138-276) ----
+ * The 2^n state lives in pinned host memory, split into 2^(n-m) tiles of
+ * 2^m amplitudes (m = tile_qubits low qubits). The gate list is cut into
+ * segments whose gates touch few enough high qubits (>= m) that the tiles a
+ * segment couples fit the device; each segment gathers every such tile
+ * group into device memory (high qubit H[r] -> local qubit m + r), runs the
+ * segment there as one compiled plan, and scatters the group back: one read
+ * and one write of the host state per segment, copies overlapped with
+ * compute over `depth` device buffers (1 = no overlap; 0 = the default 3).
+ * Errors as the reference's run_paged: EmptyCircuit for n = 0 and no
+ * instructions; InvalidState unless 1 <= tile_qubits < num_qubits;
+ * UnsupportedInstruction for measure / reset / diagonal-phase / tiled-block;
+ * TooManyQubits when tile_qubits plus the high qubits of one gate exceed
+ * what the device holds; then the in-core stream's gate validation. FP64
+ * handles keep complex128 tiles, the others complex64 (TC32 segments run
+ * their block passes without the final renormalisation). */
+typedef struct aleph_b200_paged_state aleph_b200_paged_state;
+typedef struct aleph_b200_paged_info {
+  uint32_t num_qubits;
+  uint32_t tile_qubits;     /* m */
+  uint32_t local_qubits;    /* the largest tile group on the device: m + its high qubits */
+  uint32_t depth;           /* device buffers in the ring */
+  uint64_t segments;        /* sweeps over the host state */
+  uint64_t groups;          /* tile groups gathered, computed and scattered */
+  uint64_t h2d_bytes, d2h_bytes;
+  double seconds;           /* wall time of the run, host allocation excluded */
+} aleph_b200_paged_info;
+int aleph_b200_paged_run(aleph_b200_handle* h, uint32_t num_qubits, const aleph_b200_instr* instrs, uint64_t count,
+                         const aleph_b200_pools* pools, uint32_t tile_qubits, uint32_t depth,
+                         aleph_b200_paged_state** out);
+int aleph_b200_paged_info_get(const aleph_b200_paged_state* ps, aleph_b200_paged_info* out);
+/* Interleaved (re, im) doubles, 2 * 2^n values (PagedSvState::amplitudes_vec, paged.rs:78-87). */
+int aleph_b200_paged_get_amplitudes(const aleph_b200_paged_state* ps, double* out);
+/* Sum of |a|^2 in FP64 over the host state (PagedSvState::norm_sqr, paged.rs:89-100). */
+int aleph_b200_paged_norm_sqr(const aleph_b200_paged_state* ps, double* out);
+int aleph_b200_paged_free(aleph_b200_paged_state* ps);
 
 #ifdef __cplusplus
 }
