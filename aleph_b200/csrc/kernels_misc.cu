@@ -96,56 +96,80 @@ cudaError_t launch_smem_pass(void* amps, int precision, uint32_t n, const Op* op
 }
 
 // ---- dense k-qubit op on arbitrary qubits (UnitaryKq, k = 3..5) --------------
-template <typename Real>
+// One thread per group of 2^K amplitudes (the K target bits varied, the rest
+// fixed); consecutive threads take consecutive groups, so every load and store
+// is coalesced along the lowest non-target qubits. K is a template parameter:
+// the group stays in registers and the 2^K x 2^K product unrolls (the matrix
+// is read from shared memory as warp-uniform broadcasts).
+template <typename Real, int K>
 __global__ void __launch_bounds__(256) kq_kernel(V2<Real>* __restrict__ amps, uint32_t n, const Op* __restrict__ op_p,
                                                  const V2<Real>* __restrict__ coef) {
-  __shared__ V2<Real> msm[32 * 32];
-  __shared__ uint64_t offs[32];
+  constexpr uint32_t DIM = 1u << K;
+  __shared__ V2<Real> msm[DIM * DIM];
+  __shared__ uint64_t offs[DIM];
   const Op op = *op_p;
-  const int k = op.nq;
-  const uint32_t dim = 1u << k;
-  for (uint32_t i = threadIdx.x; i < dim * dim; i += blockDim.x) msm[i] = ld_coef<Real>(coef + op.coef + i);
-  if (threadIdx.x < dim) {
+  for (uint32_t i = threadIdx.x; i < DIM * DIM; i += blockDim.x) msm[i] = ld_coef<Real>(coef + op.coef + i);
+  if (threadIdx.x < DIM) {
     uint64_t o = 0;
-    for (int p = 0; p < k; ++p)
-      if ((threadIdx.x >> p) & 1) o |= 1ull << op.q[k - 1 - p];
+#pragma unroll
+    for (int p = 0; p < K; ++p)
+      if ((threadIdx.x >> p) & 1) o |= 1ull << op.q[K - 1 - p];
     offs[threadIdx.x] = o;
   }
   __syncthreads();
-  uint32_t sorted[6];
-  for (int i = 0; i < k; ++i) sorted[i] = op.q[i];
-  for (int i = 1; i < k; ++i)
-    for (int j = i; j > 0 && sorted[j - 1] > sorted[j]; --j) {
-      uint32_t t = sorted[j];
-      sorted[j] = sorted[j - 1];
-      sorted[j - 1] = t;
-    }
-  const uint64_t groups = 1ull << (n - k);
+  uint32_t sorted[K];
+#pragma unroll
+  for (int i = 0; i < K; ++i) sorted[i] = op.q[i];
+#pragma unroll
+  for (int i = 1; i < K; ++i)
+#pragma unroll
+    for (int j = i; j > 0; --j)
+      if (sorted[j - 1] > sorted[j]) {
+        const uint32_t t = sorted[j];
+        sorted[j] = sorted[j - 1];
+        sorted[j - 1] = t;
+      }
+  const uint64_t groups = 1ull << (n - K);
   for (uint64_t gi = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; gi < groups;
        gi += (uint64_t)gridDim.x * blockDim.x) {
     uint64_t base = gi;
-    for (int i = 0; i < k; ++i) base = insert_zero(base, sorted[i]);
+#pragma unroll
+    for (int i = 0; i < K; ++i) base = insert_zero(base, sorted[i]);
     if ((base & op.ctrl) != op.ctrl) continue;
-    V2<Real> x[32];
-    for (uint32_t c = 0; c < dim; ++c) x[c] = ld_amp<Real>(amps + (base | offs[c]));
-    for (uint32_t r = 0; r < dim; ++r) {
+    V2<Real> x[DIM];
+#pragma unroll
+    for (uint32_t c = 0; c < DIM; ++c) x[c] = ld_amp<Real>(amps + (base | offs[c]));
+#pragma unroll
+    for (uint32_t r = 0; r < DIM; ++r) {
       V2<Real> acc = mk<Real>(0, 0);
-      for (uint32_t c = 0; c < dim; ++c) acc = cadd<Real>(acc, cmul<Real>(msm[r * dim + c], x[c]));
+#pragma unroll
+      for (uint32_t c = 0; c < DIM; ++c) acc = cadd<Real>(acc, cmul<Real>(msm[r * DIM + c], x[c]));
       st_amp<Real>(amps + (base | offs[r]), acc);
     }
   }
 }
 
+template <typename Real>
+cudaError_t launch_kq_typed(V2<Real>* amps, uint32_t n, const Op* op_dev, uint32_t k, const V2<Real>* coef,
+                            unsigned blocks, cudaStream_t s) {
+  switch (k) {
+    case 3: kq_kernel<Real, 3><<<blocks, 256, 0, s>>>(amps, n, op_dev, coef); break;
+    case 4: kq_kernel<Real, 4><<<blocks, 256, 0, s>>>(amps, n, op_dev, coef); break;
+    case 5: kq_kernel<Real, 5><<<blocks, 256, 0, s>>>(amps, n, op_dev, coef); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
 cudaError_t launch_kq_pass(void* amps, int precision, uint32_t n, const Op* op_dev, const Op& op_host,
                            const void* coef, cudaStream_t s) {
+  if (op_host.nq < 3 || op_host.nq > 5 || n < op_host.nq) return cudaErrorInvalidValue;
   const uint64_t groups = 1ull << (n - op_host.nq);
   const uint64_t blocks64 = (groups + 255) / 256;
   const unsigned blocks = (unsigned)(blocks64 > 148ull * 16 ? 148ull * 16 : blocks64);
   if (precision == ALEPH_B200_F64)
-    kq_kernel<double><<<blocks, 256, 0, s>>>((double2*)amps, n, op_dev, (const double2*)coef);
-  else
-    kq_kernel<float><<<blocks, 256, 0, s>>>((float2*)amps, n, op_dev, (const float2*)coef);
-  return cudaGetLastError();
+    return launch_kq_typed<double>((double2*)amps, n, op_dev, op_host.nq, (const double2*)coef, blocks, s);
+  return launch_kq_typed<float>((float2*)amps, n, op_dev, op_host.nq, (const float2*)coef, blocks, s);
 }
 
 // ---- state initialisation / conversion / permutation ------------------------

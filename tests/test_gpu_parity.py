@@ -96,6 +96,24 @@ def test_random_all_gates_f64(n, smem, tile_r):
     assert np.abs(got - want).max() <= F64_TOL
 
 
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+@pytest.mark.parametrize("k", [3, 4, 5])
+def test_dense_kq_pass(k, precision):
+    """UnitaryKq (k = 3..5) runs as its own dense k-qubit pass: scattered
+    targets in any order (lowest qubit in and out of the set), against the
+    oracle. (The reference rejects controls on UnitaryKq.)"""
+    n = 15
+    rng = np.random.default_rng(60 + k)
+    c = workloads.brickwall(n, 2, seed=61)
+    for first in (0, 9):
+        qs = [first] + [int(q) for q in rng.permutation([q for q in range(n) if q != first])[: k - 1]]
+        z = rng.standard_normal((2**k, 2**k)) + 1j * rng.standard_normal((2**k, 2**k))
+        c.add(C.UnitaryKq(np.linalg.qr(z)[0]), qs)
+    got, _, be, _ = engine_state(c, precision=precision)
+    want, _ = oracle.run(n, c.instructions)
+    assert np.abs(got - want).max() <= (F64_TOL if precision == "f64" else F32_TOL)
+
+
 @pytest.mark.parametrize("n", [8, 14, 20])
 def test_brickwall_f64(n):
     c = workloads.brickwall(n, 20, seed=1)
