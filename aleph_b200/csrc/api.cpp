@@ -928,14 +928,22 @@ int aleph_b200_paged_run(aleph_b200_handle* h, uint32_t n, const aleph_b200_inst
   std::memset(ps->host, 0, ps->bytes);
   if (prec == ALEPH_B200_F64) ((double*)ps->host)[0] = 1.0;
   else ((float*)ps->host)[0] = 1.0f;
+  PagedRing ring;
+  ring.device = h->device;
+  Scratch plan_buf;  // the current segment's uploaded plan tables
+  // on failure: no copy into or out of the host state may still be in
+  // flight when it is freed
   auto fail = [&](int r) {
+    if (ring.h2d) cudaStreamSynchronize(ring.h2d);
+    if (ring.d2h) cudaStreamSynchronize(ring.d2h);
+    cudaStreamSynchronize(h->stream);
+    if (plan_buf.ptr) cudaFree(plan_buf.ptr);
+    plan_buf = Scratch{};
     aleph_b200_paged_free(ps);
     return r;
   };
   const auto t0 = std::chrono::steady_clock::now();
 
-  PagedRing ring;
-  ring.device = h->device;
   const size_t buf_bytes = bpa << l_used;
   ring.buf.assign(depth, nullptr);
   ring.in.assign(depth, nullptr);
@@ -984,7 +992,6 @@ int aleph_b200_paged_run(aleph_b200_handle* h, uint32_t n, const aleph_b200_inst
       if (int s = build_plan(ops, nl, h->opts, &P)) return fail(set_error(h, s, "optimization pipeline failed: planner"));
       P.renormalize = false;
     }
-    Scratch plan_buf;
     bool uploaded = false;
     // tile index bit (q - m) <-> qubit q
     std::vector<uint32_t> hbit(hh), rbit(R.size());
@@ -1031,10 +1038,7 @@ int aleph_b200_paged_run(aleph_b200_handle* h, uint32_t n, const aleph_b200_inst
       st.precision = prec;
       st.amps = ring.buf[slot];
       st.bytes = bpa << nl;
-      if (int r = run_plan(h, &st, P, nullptr, 0, nullptr, 0, nullptr, nullptr, &plan_buf, &uploaded)) {
-        if (plan_buf.ptr) cudaFree(plan_buf.ptr);
-        return fail(r);
-      }
+      if (int r = run_plan(h, &st, P, nullptr, 0, nullptr, 0, nullptr, nullptr, &plan_buf, &uploaded)) return fail(r);
       CK_OR(cudaEventRecord(ring.done[slot], h->stream), fail, "event record");
       CK_OR(cudaStreamWaitEvent(ring.d2h, ring.done[slot], 0), fail, "stream wait");
       CK_OR(copies(o, slot, false), fail, "paged scatter");
@@ -1046,6 +1050,7 @@ int aleph_b200_paged_run(aleph_b200_handle* h, uint32_t n, const aleph_b200_inst
     ++info.segments;
     cudaStreamSynchronize(h->stream);
     if (plan_buf.ptr) cudaFree(plan_buf.ptr);
+    plan_buf = Scratch{};
   }
   CK_OR(cudaStreamSynchronize(ring.d2h), fail, "stream synchronize");
   CK_OR(cudaStreamSynchronize(ring.h2d), fail, "stream synchronize");
