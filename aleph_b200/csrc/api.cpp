@@ -1079,16 +1079,26 @@ int aleph_b200_paged_get_amplitudes(const aleph_b200_paged_state* ps, double* ou
 
 int aleph_b200_paged_norm_sqr(const aleph_b200_paged_state* ps, double* out) {
   if (!ps || !out) return ALEPH_B200_INVALID_ARGUMENT;
-  const uint64_t len = 1ull << ps->n;
-  double s = 0.0;
-  if (ps->precision == ALEPH_B200_F64) {
-    const double* d = (const double*)ps->host;
-    for (uint64_t i = 0; i < 2 * len; ++i) s += d[i] * d[i];
-  } else {
-    const float* f = (const float*)ps->host;
-    for (uint64_t i = 0; i < 2 * len; ++i) s += (double)f[i] * (double)f[i];
+  // blocks of 4096 squares summed plainly, block sums added with Kahan
+  // compensation: the rounding error stays near that of one block, not of
+  // a 2^(n+1)-term running sum
+  const uint64_t count = 2ull << ps->n;
+  double total = 0.0, comp = 0.0;
+  for (uint64_t b = 0; b < count; b += 4096) {
+    const uint64_t e = std::min<uint64_t>(count, b + 4096);
+    double blk = 0.0;
+    if (ps->precision == ALEPH_B200_F64) {
+      const double* d = (const double*)ps->host;
+      for (uint64_t i = b; i < e; ++i) blk += d[i] * d[i];
+    } else {
+      const float* f = (const float*)ps->host;
+      for (uint64_t i = b; i < e; ++i) blk += (double)f[i] * (double)f[i];
+    }
+    const double y = blk - comp, t = total + y;
+    comp = (t - total) - y;
+    total = t;
   }
-  *out = s;
+  *out = total;
   return ALEPH_B200_OK;
 }
 

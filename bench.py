@@ -397,6 +397,29 @@ def qaoa_sweep_bench(dev: int, sets: int, loop_sample: int, seed: int) -> dict:
     return out
 
 
+def out_of_core_bench(dev: int, seed: int, n: int = 28, depth: int = 4, tile_qubits: int = 20,
+                      local_qubits: int = 26) -> dict:
+    """The out-of-core path (aleph_b200_paged_run): an FP64 brickwall whose
+    state lives in pinned host memory, streamed through the device in tile
+    groups of at most 2^local_qubits amplitudes (1 GiB at 26), three device
+    buffers in the ring. Reports the host<->device traffic rate."""
+    from aleph_b200 import workloads
+    from aleph_b200.backend import B200SvBackend
+
+    be = B200SvBackend(seed=0, device=dev, precision="f64").set_tuning("paged_local_qubits", local_qubits)
+    c = workloads.brickwall(n, depth, seed=seed)
+    ps = be.run_paged(c, tile_qubits, depth=3)
+    info = ps.info()
+    norm = ps.norm_sqr()
+    ps.free()
+    be.close()
+    moved = info["h2d_bytes"] + info["d2h_bytes"]
+    return {"workload": f"brickwall n={n} depth={depth}, FP64, host-resident state", "tile_qubits": tile_qubits,
+            "local_qubits": info["local_qubits"], "segments": info["segments"], "groups": info["groups"],
+            "bytes_moved": moved, "seconds": round(info["seconds"], 4),
+            "host_device_gbs": round(moved / info["seconds"] / 1e9, 1), "norm_sqr": norm}
+
+
 def small_configs_bench(dev: int, seed: int, greedy: bool = False) -> dict:
     """The two plain-FP64 configurations beside the headline:
     C0: brickwall n=20 depth 20, full state and 1024 shots against the oracle;
@@ -576,6 +599,9 @@ def run_engine(args, ranks: Ranks):
     small = None
     if not args.skip_small and ranks.rank == 0:
         small = small_configs_bench(dev, args.seed, greedy=args.greedy)
+    paged = None
+    if not args.skip_paged and ranks.rank == 0:
+        paged = out_of_core_bench(dev, args.seed)
 
     cpu = None
     if ranks.world == 1 and not args.skip_cpu:
@@ -595,7 +621,7 @@ def run_engine(args, ranks: Ranks):
             "clocks": clk, "e2e": e2e, "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu,
             "kernels": table, "fp64_plain": fp64, "fidelity": fid, "final_norm_sqr": norm,
             "plan_choice": None if choice is None else dict(choice.__dict__, source="learned cost model"),
-            "qaoa_sweep": qaoa, "fp64_configs": small,
+            "qaoa_sweep": qaoa, "fp64_configs": small, "out_of_core": paged,
         }
         print(json.dumps(line), flush=True)
     ranks.close()
@@ -634,6 +660,7 @@ def main(argv=None):
     ap.add_argument("--qaoa-sets", type=int, default=4096, help="QAOA sweep size (0: skip)")
     ap.add_argument("--greedy", action="store_true", help="the greedy plan configuration, no cost model")
     ap.add_argument("--skip-small", action="store_true", help="skip the n=20 brickwall / n=30 QFT FP64 checks")
+    ap.add_argument("--skip-paged", action="store_true", help="skip the out-of-core (host-paged) run")
     args = ap.parse_args(argv)
     args.warmup = max(3, args.warmup)  # at least 3 untimed warm-up steps
     ranks = Ranks()

@@ -440,7 +440,7 @@ int aleph_b200_paged_run(aleph_b200_handle* h, uint32_t num_qubits, const aleph_
 int aleph_b200_paged_info_get(const aleph_b200_paged_state* ps, aleph_b200_paged_info* out);
 /* Interleaved (re, im) doubles, 2 * 2^n values (PagedSvState::amplitudes_vec, paged.rs:78-87). */
 int aleph_b200_paged_get_amplitudes(const aleph_b200_paged_state* ps, double* out);
-/* Sum of |a|^2 in FP64 over the host state (PagedSvState::norm_sqr, paged.rs:89-100). */
+/* Sum of |a|^2 in FP64 over the host state, block sums Kahan-compensated (PagedSvState::norm_sqr, paged.rs:89-100). */
 int aleph_b200_paged_norm_sqr(const aleph_b200_paged_state* ps, double* out);
 int aleph_b200_paged_free(aleph_b200_paged_state* ps);
 
