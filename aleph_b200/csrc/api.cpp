@@ -925,9 +925,15 @@ int aleph_b200_paged_run(aleph_b200_handle* h, uint32_t n, const aleph_b200_inst
     delete ps;
     return cuda_fail(h, ce, "pinned host state allocation");
   }
-  std::memset(ps->host, 0, ps->bytes);
-  if (prec == ALEPH_B200_F64) ((double*)ps->host)[0] = 1.0;
-  else ((float*)ps->host)[0] = 1.0f;
+  // The first segment generates |0...0> on the device and its scatters write
+  // every tile, so the host state is only initialised when no gate runs.
+  if (segs.empty()) {
+    std::memset(ps->host, 0, ps->bytes);
+    if (prec == ALEPH_B200_F64) ((double*)ps->host)[0] = 1.0;
+    else ((float*)ps->host)[0] = 1.0f;
+  }
+  static const double kOne64[2] = {1.0, 0.0};
+  static const float kOne32[2] = {1.0f, 0.0f};
   PagedRing ring;
   ring.device = h->device;
   Scratch plan_buf;  // the current segment's uploaded plan tables
@@ -1015,13 +1021,23 @@ int aleph_b200_paged_run(aleph_b200_handle* h, uint32_t n, const aleph_b200_inst
     // gather of group g (outer index o): waits for the slot's previous scatter
     // and, for a segment's first group, for every scatter of the segment
     // before (the tiles it reads were written there; d2h is in order)
+    // (the first segment generates its groups: zeros, and amplitude 1 at
+    // index 0, which sits at offset 0 of outer group 0)
+    const bool generate = si == 0;
     auto gather = [&](uint64_t g, uint64_t o, bool first_of_segment) -> cudaError_t {
       const uint32_t slot = (uint32_t)(g % depth);
       cudaError_t e = cudaSuccess;
       if (g >= depth) e = cudaStreamWaitEvent(ring.h2d, ring.out[slot], 0);
       if (e == cudaSuccess && first_of_segment && g > 0)
         e = cudaStreamWaitEvent(ring.h2d, ring.out[(g - 1) % depth], 0);
-      if (e == cudaSuccess) e = copies(o, slot, true);
+      if (e == cudaSuccess && generate) {
+        e = cudaMemsetAsync(ring.buf[slot], 0, n_sub * tile_bytes, ring.h2d);
+        if (e == cudaSuccess && o == 0)
+          e = cudaMemcpyAsync(ring.buf[slot], prec == ALEPH_B200_F64 ? (const void*)kOne64 : (const void*)kOne32, bpa,
+                              cudaMemcpyHostToDevice, ring.h2d);
+      } else if (e == cudaSuccess) {
+        e = copies(o, slot, true);
+      }
       if (e == cudaSuccess) e = cudaEventRecord(ring.in[slot], ring.h2d);
       return e;
     };

@@ -30,8 +30,10 @@ def test_paged_f64_matches_the_oracle(n, m, local):
     info = ps.info()
     assert info["tile_qubits"] == m and info["local_qubits"] <= local
     assert info["segments"] > 1 and info["groups"] > info["segments"]
-    # every segment reads and writes the whole host state exactly once
-    assert info["h2d_bytes"] == info["d2h_bytes"] == info["segments"] * (16 << n)
+    # every segment writes the whole host state once; every segment after the
+    # first reads it once (the first generates |0...0> on the device)
+    assert info["d2h_bytes"] == info["segments"] * (16 << n)
+    assert info["h2d_bytes"] == (info["segments"] - 1) * (16 << n)
     ps.free()
     be.close()
 
