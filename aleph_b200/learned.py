@@ -10,7 +10,7 @@ times of the passes each one would launch (``describe_plan``, host only), in
 place of the fixed greedy configuration. ``autotune`` keeps a learned choice
 only when it is measured faster than the greedy plan and its final state
 matches the greedy plan's within the precision's tolerance: the greedy plan
-stays the fallback and the judge.
+stays the fallback and the yardstick.
 
 The reference has no counterpart: its fusion is the greedy FuseKq heuristic
 (crates/aleph-ir/src/passes/fuse_kq.rs:268-400).
