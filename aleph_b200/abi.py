@@ -246,6 +246,9 @@ _SIGNATURES = {
     "aleph_b200_paged_get_amplitudes": ([_P, ct.POINTER(ct.c_double)], ct.c_int),
     "aleph_b200_paged_norm_sqr": ([_P, ct.POINTER(ct.c_double)], ct.c_int),
     "aleph_b200_paged_free": ([_P], ct.c_int),
+    "aleph_b200_describe_paged": (
+        [ct.c_uint32, ct.POINTER(Instr), ct.c_uint64, ct.c_uint32, ct.c_uint32, ct.POINTER(ct.c_uint64),
+         ct.POINTER(ct.c_uint64), ct.POINTER(ct.c_uint64)], ct.c_int),
 }
 
 _LIB = None

@@ -405,6 +405,23 @@ def describe_plan(num_qubits: int, instructions, precision: str = "f64", tile_r:
     return [_record_dict(r) for r in buf[: n.value]]
 
 
+def describe_paged(num_qubits: int, instructions, tile_qubits: int, local_qubits: int):
+    """How an out-of-core run cuts ``instructions`` (host only, no device):
+    (segment of each instruction, its place in the execution order, segment
+    count); barriers get -1 in both lists."""
+    lib = abi.load_library()
+    flat = instructions if isinstance(instructions, Flat) else flatten(instructions)
+    seg = (ct.c_uint64 * max(1, flat.n))()
+    pos = (ct.c_uint64 * max(1, flat.n))()
+    count = ct.c_uint64()
+    st = lib.aleph_b200_describe_paged(num_qubits, flat.instrs, flat.n, tile_qubits, local_qubits, seg, pos,
+                                       ct.byref(count))
+    if st != abi.OK:
+        raise _ERRORS.get(st, BackendError)(st, f"describe_paged: {abi.STATUS_NAMES.get(st, st)}")
+    conv = lambda v: -1 if v == 2**64 - 1 else int(v)  # noqa: E731
+    return [conv(seg[i]) for i in range(flat.n)], [conv(pos[i]) for i in range(flat.n)], count.value
+
+
 def run_with_outcomes(backend: B200SvBackend, circuit: Circuit, measure_uniforms=None):
     """``run_with_outcomes`` (crates/aleph-backend/src/lib.rs:211-245)."""
     if circuit.num_qubits == 0 and len(circuit) == 0:

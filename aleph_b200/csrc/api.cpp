@@ -794,6 +794,40 @@ uint64_t high_mask(const aleph_b200_instr& r, uint32_t m, uint32_t n) {
   return qubit_mask(r, n) & ~((1ull << m) - 1);
 }
 
+// Segments of an out-of-core run: each takes, in order, every remaining gate
+// whose high qubits (>= m) fit the budget together with the segment's, and
+// that shares no qubit with a gate the segment leaves for later, so it
+// commutes with all of them and the reordering is exact. Barriers are dropped.
+struct PagedSegment {
+  std::vector<uint64_t> gates;  // instruction indices, in execution order
+  uint64_t hmask = 0;           // the high qubits the segment gathers
+};
+std::vector<PagedSegment> paged_segments(const aleph_b200_instr* in, uint64_t count, uint32_t n, uint32_t m,
+                                         uint32_t g_budget) {
+  std::vector<PagedSegment> segs;
+  std::vector<uint64_t> remaining, deferred;
+  for (uint64_t i = 0; i < count; ++i)
+    if (in[i].kind != ALEPH_INSTR_BARRIER) remaining.push_back(i);
+  while (!remaining.empty()) {
+    PagedSegment sg;
+    uint64_t blocked = 0;
+    deferred.clear();
+    for (uint64_t i : remaining) {
+      const uint64_t qm = qubit_mask(in[i], n), gm = qm & ~((1ull << m) - 1);
+      if (!(qm & blocked) && (uint32_t)__builtin_popcountll(sg.hmask | gm) <= g_budget) {
+        sg.gates.push_back(i);
+        sg.hmask |= gm;
+      } else {
+        deferred.push_back(i);
+        blocked |= qm;
+      }
+    }
+    segs.push_back(std::move(sg));
+    remaining.swap(deferred);
+  }
+  return segs;
+}
+
 struct PagedRing {
   int device = 0;
   std::vector<void*> buf;
@@ -881,38 +915,9 @@ int aleph_b200_paged_run(aleph_b200_handle* h, uint32_t n, const aleph_b200_inst
     std::vector<Lowered> ops;
     if (int r = lower_stream(h, n, in, count, pools, &ops)) return r;
   }
-  // segments: each takes, in order, every remaining gate whose high qubits
-  // fit the budget and that shares no qubit with a gate it leaves for later
-  // (so it commutes with all of them: the reordering is exact)
-  struct Segment {
-    std::vector<uint64_t> gates;
-    uint64_t hmask;
-  };
-  std::vector<Segment> segs;
-  {
-    std::vector<uint64_t> remaining, deferred;
-    for (uint64_t i = 0; i < count; ++i)
-      if (in[i].kind != ALEPH_INSTR_BARRIER) remaining.push_back(i);
-    while (!remaining.empty()) {
-      Segment sg{{}, 0};
-      uint64_t blocked = 0;
-      deferred.clear();
-      for (uint64_t i : remaining) {
-        const uint64_t qm = qubit_mask(in[i], n), gm = qm & ~((1ull << m) - 1);
-        if (!(qm & blocked) && (uint32_t)__builtin_popcountll(sg.hmask | gm) <= g_budget) {
-          sg.gates.push_back(i);
-          sg.hmask |= gm;
-        } else {
-          deferred.push_back(i);
-          blocked |= qm;
-        }
-      }
-      segs.push_back(std::move(sg));
-      remaining.swap(deferred);
-    }
-  }
+  const std::vector<PagedSegment> segs = paged_segments(in, count, n, m, g_budget);
   uint32_t l_used = m;
-  for (const Segment& sg : segs) l_used = std::max<uint32_t>(l_used, m + (uint32_t)__builtin_popcountll(sg.hmask));
+  for (const PagedSegment& sg : segs) l_used = std::max<uint32_t>(l_used, m + (uint32_t)__builtin_popcountll(sg.hmask));
 
   aleph_b200_paged_state* ps = new (std::nothrow) aleph_b200_paged_state();
   if (!ps) return set_error(h, ALEPH_B200_DEVICE_FAILURE, "host allocation failed");
@@ -977,7 +982,7 @@ int aleph_b200_paged_run(aleph_b200_handle* h, uint32_t n, const aleph_b200_inst
   info.depth = depth;
   std::vector<aleph_b200_instr> local;
   for (size_t si = 0; si < segs.size(); ++si) {
-    const Segment& sg = segs[si];
+    const PagedSegment& sg = segs[si];
     std::vector<uint32_t> H, R;  // the segment's high qubits / the other high qubits, ascending
     for (uint32_t q = m; q < n; ++q) ((sg.hmask >> q) & 1 ? H : R).push_back(q);
     const uint32_t hh = (uint32_t)H.size(), nl = m + hh;
@@ -1122,6 +1127,33 @@ int aleph_b200_paged_free(aleph_b200_paged_state* ps) {
   if (!ps) return ALEPH_B200_OK;
   if (ps->host) cudaFreeHost(ps->host);
   delete ps;
+  return ALEPH_B200_OK;
+}
+
+int aleph_b200_describe_paged(uint32_t n, const aleph_b200_instr* in, uint64_t count, uint32_t tile_qubits,
+                              uint32_t local_qubits, uint64_t* segment_of, uint64_t* position_of,
+                              uint64_t* n_segments) {
+  if ((!in && count) || !n_segments || tile_qubits == 0 || tile_qubits >= n || n > kMaxQubits ||
+      local_qubits < tile_qubits)
+    return ALEPH_B200_INVALID_ARGUMENT;
+  uint32_t g_max = 0;
+  for (uint64_t i = 0; i < count; ++i)
+    if (in[i].kind != ALEPH_INSTR_BARRIER)
+      g_max = std::max<uint32_t>(g_max, (uint32_t)__builtin_popcountll(high_mask(in[i], tile_qubits, n)));
+  if (tile_qubits + g_max > local_qubits) return ALEPH_B200_TOO_MANY_QUBITS;
+  const std::vector<PagedSegment> segs = paged_segments(in, count, n, tile_qubits, local_qubits - tile_qubits);
+  for (uint64_t i = 0; i < count; ++i) {
+    if (segment_of) segment_of[i] = UINT64_MAX;
+    if (position_of) position_of[i] = UINT64_MAX;
+  }
+  uint64_t pos = 0;
+  for (size_t si = 0; si < segs.size(); ++si)
+    for (uint64_t i : segs[si].gates) {
+      if (segment_of) segment_of[i] = si;
+      if (position_of) position_of[i] = pos;
+      ++pos;
+    }
+  *n_segments = segs.size();
   return ALEPH_B200_OK;
 }
 

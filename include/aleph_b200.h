@@ -443,6 +443,16 @@ int aleph_b200_paged_get_amplitudes(const aleph_b200_paged_state* ps, double* ou
 /* Sum of |a|^2 in FP64 over the host state, block sums Kahan-compensated (PagedSvState::norm_sqr, paged.rs:89-100). */
 int aleph_b200_paged_norm_sqr(const aleph_b200_paged_state* ps, double* out);
 int aleph_b200_paged_free(aleph_b200_paged_state* ps);
+/* Host only, no device: how aleph_b200_paged_run would cut `instrs` for a
+ * tile split `tile_qubits` and tile groups of at most `local_qubits` qubits.
+ * segment_of[i] (optional, count entries) receives instruction i's segment
+ * and position_of[i] (optional) its place in the execution order; barriers
+ * get UINT64_MAX in both. Status TOO_MANY_QUBITS when one gate's high qubits
+ * do not fit; INVALID_ARGUMENT unless 1 <= tile_qubits < n <= 40 and
+ * local_qubits >= tile_qubits. */
+int aleph_b200_describe_paged(uint32_t num_qubits, const aleph_b200_instr* instrs, uint64_t count,
+                              uint32_t tile_qubits, uint32_t local_qubits, uint64_t* segment_of,
+                              uint64_t* position_of, uint64_t* n_segments);
 
 #ifdef __cplusplus
 }

@@ -259,3 +259,63 @@ def test_grover_workload_amplifies_the_marked_state():
         p = (np.abs(psi) ** 2).reshape(-1, 1 << nd)
         assert p[0, marked] > 0.75  # ancillas back in |0>, marked state amplified
         assert abs(p[1:].sum()) < 1e-12
+
+
+def _gate_qubits(inst):
+    return set(inst.qubits) | set(inst.controls)
+
+
+def test_paged_segments_keep_dependencies_and_budget():
+    """Out-of-core segmentation (host only): every segment gathers at most
+    local - m high qubits; gates that share a qubit keep their order; later
+    gates move ahead only across gates they share no qubit with."""
+    from aleph_b200.backend import describe_paged
+
+    for n, m, local, seed in ((16, 8, 12, 1), (20, 12, 15, 2), (12, 4, 9, 3)):
+        c = workloads.brickwall(n, 6, seed=seed)
+        c.add(C.Toffoli(), [n - 1, 0, n - 3]).add(C.Swap(), [2, n - 2])
+        seg, pos, count = describe_paged(n, c.instructions, m, local)
+        gates = c.instructions
+        assert all(s >= 0 for s in seg) and sorted(pos) == list(range(len(gates)))
+        for s in range(count):
+            high = set()
+            for i, g in enumerate(gates):
+                if seg[i] == s:
+                    high |= {q for q in _gate_qubits(g) if q >= m}
+            assert len(high) <= local - m
+        for i in range(len(gates)):
+            for j in range(i + 1, len(gates)):
+                if _gate_qubits(gates[i]) & _gate_qubits(gates[j]):
+                    assert pos[i] < pos[j] and seg[i] <= seg[j]
+        assert count < len(gates)
+
+
+def test_paged_segments_merge_across_commuting_gates():
+    """Two alternating bands of high qubits: a program-order cut would open a
+    segment per band switch; commuting gates are pulled forward instead."""
+    from aleph_b200.backend import describe_paged
+
+    n, m = 14, 6
+    c = C.Circuit(n)
+    for _ in range(6):
+        c.add(C.Cnot(), [0, 8]).add(C.Cnot(), [1, 9])      # band {8, 9}
+        c.add(C.Cnot(), [2, 12]).add(C.Cnot(), [3, 13])    # band {12, 13}
+    seg, _, count = describe_paged(n, c.instructions, m, m + 2)
+    assert count == 2
+    assert {seg[i] for i in range(0, len(seg), 4)} == {0} and {seg[i] for i in range(2, len(seg), 4)} == {1}
+    c.instructions.insert(0, C.Barrier((0, 1)))
+    seg, pos, count = describe_paged(n, c.instructions, m, m + 2)
+    assert seg[0] == -1 and pos[0] == -1 and count == 2
+
+
+def test_paged_segments_errors():
+    from aleph_b200 import backend as B
+    from aleph_b200.backend import describe_paged
+
+    c = C.Circuit(10).add(C.Toffoli(), [7, 8, 9])
+    with pytest.raises(B.TooManyQubits):
+        describe_paged(10, c.instructions, 4, 6)
+    with pytest.raises(B.InvalidArgument):
+        describe_paged(10, c.instructions, 10, 12)
+    with pytest.raises(B.InvalidArgument):
+        describe_paged(10, c.instructions, 4, 3)
