@@ -412,7 +412,17 @@ cudaError_t launch_permute_pass(void* amps, int precision, uint32_t n, const uin
 template <typename Real>
 __global__ void rescale_kernel(V2<Real>* __restrict__ amps, uint64_t len, const double* __restrict__ norm2) {
   const double s = norm2[0] > 0.0 ? rsqrt(norm2[0]) : 1.0;
-  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < len; i += (uint64_t)gridDim.x * blockDim.x) {
+  // four independent loads per step (bytes in flight, as in norm_kernel)
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  for (; i + 3 * stride < len; i += 4 * stride) {
+    V2<Real> a[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) a[k] = ld_amp<Real>(amps + i + k * stride);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) st_amp<Real>(amps + i + k * stride, mk<Real>((Real)(a[k].x * s), (Real)(a[k].y * s)));
+  }
+  for (; i < len; i += stride) {
     const V2<Real> a = ld_amp<Real>(amps + i);
     st_amp<Real>(amps + i, mk<Real>((Real)(a.x * s), (Real)(a.y * s)));
   }

@@ -66,7 +66,22 @@ template <typename Real>
 __global__ void __launch_bounds__(RB) norm_kernel(const V2<Real>* __restrict__ amps, uint64_t len,
                                                   double* __restrict__ partials) {
   double v[2] = {0.0, 0.0};
-  for (uint64_t i = (uint64_t)blockIdx.x * RB + threadIdx.x; i < len; i += (uint64_t)gridDim.x * RB) {
+  // four independent loads per step keep enough bytes in flight for the
+  // 8-byte complex64 amplitudes (one load per step left the pass latency-bound)
+  const uint64_t stride = (uint64_t)gridDim.x * RB;
+  uint64_t i = (uint64_t)blockIdx.x * RB + threadIdx.x;
+  for (; i + 3 * stride < len; i += 4 * stride) {
+    V2<Real> a[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) a[k] = ld_amp<Real>(amps + i + k * stride);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const double p = abs2<Real>(a[k]);
+      if (isfinite(p)) v[0] += p;
+      else v[1] += 1.0;
+    }
+  }
+  for (; i < len; i += stride) {
     const double p = abs2<Real>(ld_amp<Real>(amps + i));
     if (isfinite(p)) v[0] += p;
     else v[1] += 1.0;
