@@ -104,12 +104,21 @@ template <typename Real>
 __global__ void __launch_bounds__(RB) branch_kernel(const V2<Real>* __restrict__ amps, uint64_t len, uint64_t qb,
                                                     double* __restrict__ partials) {
   double v[3] = {0.0, 0.0, 0.0};
-  for (uint64_t i = (uint64_t)blockIdx.x * RB + threadIdx.x; i < len; i += (uint64_t)gridDim.x * RB) {
-    const double p = abs2<Real>(ld_amp<Real>(amps + i));
+  auto add = [&](uint64_t i, double p) {
     if (!isfinite(p)) v[2] += 1.0;
     else if (i & qb) v[1] += p;
     else v[0] += p;
+  };
+  const uint64_t stride = (uint64_t)gridDim.x * RB;
+  uint64_t i = (uint64_t)blockIdx.x * RB + threadIdx.x;
+  for (; i + 3 * stride < len; i += 4 * stride) {  // four loads in flight per step (see norm_kernel)
+    V2<Real> a[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) a[k] = ld_amp<Real>(amps + i + k * stride);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) add(i + k * stride, abs2<Real>(a[k]));
   }
+  for (; i < len; i += stride) add(i, abs2<Real>(ld_amp<Real>(amps + i)));
   block_reduce_store<3>(v, partials + 3 * blockIdx.x);
 }
 
@@ -256,7 +265,28 @@ __global__ void __launch_bounds__(RB) pauli_group_kernel(const V2<Real>* __restr
   double v[2 + PauliGroup::MAX_TERMS];
 #pragma unroll
   for (int k = 0; k < 2 + PauliGroup::MAX_TERMS; ++k) v[k] = 0.0;
-  for (uint64_t i = (uint64_t)blockIdx.x * RB + threadIdx.x; i < len; i += (uint64_t)gridDim.x * RB) {
+  const uint64_t stride = (uint64_t)gridDim.x * RB;
+  uint64_t i0 = (uint64_t)blockIdx.x * RB + threadIdx.x;
+  if constexpr (DIAG) {  // no X/Y factor: Re conj(a) a = |a|^2 and ny = 0
+    auto add = [&](uint64_t i, double p) {
+      if (!isfinite(p)) {
+        v[1] += 1.0;
+        return;
+      }
+      v[0] += p;
+#pragma unroll
+      for (int k = 0; k < PauliGroup::MAX_TERMS; ++k)
+        if (k < (int)g.count) v[2 + k] += (__popcll(g.zmask[k] & i) & 1) ? -p : p;
+    };
+    for (; i0 + 3 * stride < len; i0 += 4 * stride) {  // four loads in flight per step (see norm_kernel)
+      V2<Real> a[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) a[k] = ld_amp<Real>(amps + i0 + k * stride);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) add(i0 + k * stride, abs2<Real>(a[k]));
+    }
+  }
+  for (uint64_t i = i0; i < len; i += stride) {
     const V2<Real> a = ld_amp<Real>(amps + i);
     const double p = abs2<Real>(a);
     if (!isfinite(p)) {
@@ -264,7 +294,7 @@ __global__ void __launch_bounds__(RB) pauli_group_kernel(const V2<Real>* __restr
       continue;
     }
     v[0] += p;
-    if constexpr (DIAG) {  // no X/Y factor: Re conj(a) a = |a|^2 and ny = 0
+    if constexpr (DIAG) {
 #pragma unroll
       for (int k = 0; k < PauliGroup::MAX_TERMS; ++k)
         if (k < (int)g.count) v[2 + k] += (__popcll(g.zmask[k] & i) & 1) ? -p : p;
