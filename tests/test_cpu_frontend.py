@@ -233,6 +233,8 @@ def test_pauli_sum_text_format():
         "0.5 ZZZ\n": "line 1: pauli string has 3 chars, expected 2",
         "0.5 ZA\n": "line 1: 'A' is not one of I,X,Y,Z",
         "inf ZZ\n": "line 1: non-finite coefficient",
+        "0.5\tZZ\tX\n": "line 1: expected '<coeff> <pauli>', got \"0.5\\tZZ\\tX\"",  # Rust {:?} escapes
+        '0.5 Z"\n': "line 1: '\"' is not one of I,X,Y,Z",  # a char's {:?} keeps '"' bare
     }
     for src, msg in bad.items():
         with pytest.raises(frontend.PauliSumError) as e:
