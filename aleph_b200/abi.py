@@ -126,6 +126,8 @@ class Stats(ct.Structure):
         ("algorithmic_bytes", ct.c_double),
         ("h2d_bytes", ct.c_uint64),
         ("d2h_bytes", ct.c_uint64),
+        ("guard_band_shots", ct.c_uint64),
+        ("guard_band_inexact", ct.c_uint64),
     ]
 
 
@@ -211,6 +213,7 @@ _SIGNATURES = {
          ct.c_uint64, ct.POINTER(ct.c_double), ct.POINTER(ct.c_double)], ct.c_int),
     "aleph_b200_probabilities": ([_P, _P, ct.POINTER(ct.c_uint32), ct.c_uint32, ct.POINTER(ct.c_double)], ct.c_int),
     "aleph_b200_get_amplitudes": ([_P, _P, ct.POINTER(ct.c_double)], ct.c_int),
+    "aleph_b200_get_amplitude_range": ([_P, _P, ct.c_uint64, ct.c_uint64, ct.POINTER(ct.c_double)], ct.c_int),
     "aleph_b200_set_amplitudes": ([_P, _P, ct.POINTER(ct.c_double)], ct.c_int),
     "aleph_b200_norm_sqr": ([_P, _P, ct.POINTER(ct.c_double)], ct.c_int),
     "aleph_b200_synchronize": ([_P], ct.c_int),

@@ -251,6 +251,13 @@ class B200SvBackend:
                                                        out.ctypes.data_as(ct.POINTER(ct.c_double))))
         return out[0::2] + 1j * out[1::2]
 
+    def amplitude_range(self, state: State, first: int, count: int) -> np.ndarray:
+        """Amplitudes [first, first + count) of a state of any size."""
+        out = np.zeros(2 * max(1, count), dtype=np.float64)
+        self._check(self.lib.aleph_b200_get_amplitude_range(self.handle, state.ptr, first, count,
+                                                            out.ctypes.data_as(ct.POINTER(ct.c_double))))
+        return out[0:2 * count:2] + 1j * out[1:2 * count:2]
+
     def set_statevector(self, state: State, psi) -> None:
         psi = np.asarray(psi, dtype=np.complex128)
         buf = np.empty(2 * psi.size, dtype=np.float64)

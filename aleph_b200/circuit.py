@@ -252,6 +252,9 @@ def flatten(instructions: Sequence) -> Flat:
         elif isinstance(inst, Barrier):
             r = abi.Instr()
             r.kind = abi.INSTR_BARRIER
+            r.num_qubits = len(inst.qubits)
+            for q in inst.qubits:
+                r.data_offset |= 1 << int(q)
             recs.append(r)
         elif isinstance(inst, DiagonalPhase):
             r = abi.Instr()

@@ -392,7 +392,16 @@ int aleph_b200_create(uint64_t seed, int device, int precision, aleph_b200_handl
   cudaError_t e = cudaSetDevice(device);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, device);
+  // Load the sampling module now, which reserves the fixed buffer of
+  // aleph_b200_sample_cumulative_noalloc on this device: under lazy module
+  // loading it would otherwise be reserved at that entry point's first call,
+  // when the device may already be full.
+  if (e == cudaSuccess) {
+    void* fixed = nullptr;
+    e = fixed_sample_scratch_address(&fixed);
+  }
   if (e != cudaSuccess) {
+    if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return ALEPH_B200_DEVICE_FAILURE;
   }
@@ -578,6 +587,7 @@ static int lower_stream(aleph_b200_handle* h, uint32_t n, const aleph_b200_instr
   std::vector<uint32_t> phys(n);
   for (uint32_t q = 0; q < n; ++q) phys[q] = q;
   uint32_t swaps = 0;  // SWAP records absorbed since the map was last settled
+  uint64_t tiled_left = 0;  // gates of the current TiledBlock record still to come
   auto mapped = [&]() {
     for (uint32_t q = 0; q < n; ++q)
       if (phys[q] != q) return true;
@@ -587,9 +597,17 @@ static int lower_stream(aleph_b200_handle* h, uint32_t n, const aleph_b200_instr
     const aleph_b200_instr& g = in[i];
     aleph_b200_error_info e{};
     e.instruction = (uint32_t)i;
+    const bool tiled = tiled_left > 0;
+    if (tiled) --tiled_left;
+    if (tiled && g.kind >= 28) {
+      // a TiledBlock holds gates only (crates/aleph-ir/src/tiled_block.rs)
+      e.status = ALEPH_B200_INVALID_ARGUMENT;
+      std::snprintf(e.kind, sizeof(e.kind), "tiled block member");
+      return report(h, e);
+    }
     if (g.kind < 28) {
       ops.emplace_back();
-      if (lower_gate(g, n, pool, pool_len, &ops.back(), &e)) return report(h, e);
+      if (lower_gate(g, n, pool, pool_len, &ops.back(), &e, tiled)) return report(h, e);
       ops.back().record = (uint32_t)i;
       if (relabel && g.kind == ALEPH_GATE_SWAP && g.num_controls == 0) {
         ops.pop_back();  // validated; the swap becomes a relabeling
@@ -602,7 +620,7 @@ static int lower_stream(aleph_b200_handle* h, uint32_t n, const aleph_b200_instr
         for (uint32_t k = 0; k < g.num_qubits && k < 8; ++k) gm.qubits[k] = phys[g.qubits[k]];
         for (uint32_t k = 0; k < g.num_controls && k < 8; ++k) gm.controls[k] = phys[g.controls[k]];
         ops.back() = Lowered{};
-        if (lower_gate(gm, n, pool, pool_len, &ops.back(), &e)) return report(h, e);
+        if (lower_gate(gm, n, pool, pool_len, &ops.back(), &e, tiled)) return report(h, e);
         ops.back().record = (uint32_t)i;
       }
     } else if (g.kind == ALEPH_INSTR_MEASURE) {
@@ -626,8 +644,20 @@ static int lower_stream(aleph_b200_handle* h, uint32_t n, const aleph_b200_instr
       e.status = ALEPH_B200_UNSUPPORTED_INSTRUCTION;
       std::snprintf(e.kind, sizeof(e.kind), "reset");
       return report(h, e);
-    } else if (g.kind == ALEPH_INSTR_BARRIER || g.kind == ALEPH_INSTR_TILED_BLOCK) {
-      continue;  // barrier: no-op; tiled block: its gates follow as plain records
+    } else if (g.kind == ALEPH_INSTR_BARRIER) {
+      continue;  // no-op
+    } else if (g.kind == ALEPH_INSTR_TILED_BLOCK) {
+      // its data_len gates follow as plain records; controls at or above
+      // tile_bits act as ordinary controls (the reference's executor skips
+      // the tiles where they are 0, backend.rs:239-261), so the gates are
+      // planned like any others
+      if (g.data_len > count - i - 1) {
+        e.status = ALEPH_B200_INVALID_ARGUMENT;
+        std::snprintf(e.kind, sizeof(e.kind), "tiled block length");
+        return report(h, e);
+      }
+      tiled_left = g.data_len;
+      continue;
     } else if (g.kind == ALEPH_INSTR_DIAGONAL_PHASE) {
       if (!pools || g.data_offset + g.data_len > pools->n_terms || (g.data_len && !pools->terms)) {
         e.status = ALEPH_B200_INVALID_ARGUMENT;
@@ -859,7 +889,7 @@ int aleph_b200_paged_run(aleph_b200_handle* h, uint32_t n, const aleph_b200_inst
   if (m == 0 || m >= n) {
     aleph_b200_error_info e{};
     e.status = ALEPH_B200_INVALID_STATE;
-    std::snprintf(e.kind, sizeof(e.kind), "paged tile_qubits must satisfy 1 <= tile_qubits < num_qubits");
+    std::snprintf(e.kind, sizeof(e.kind), "paged: need 1<=tile_qubits<n");
     return report(h, e);
   }
   if (n > kMaxQubits) {
@@ -1377,6 +1407,12 @@ static int check_norm_host(aleph_b200_handle* h, aleph_b200_state* st, double* n
   return 0;
 }
 
+// status[2] of a CUMULATIVE sampling call: its shots inside the guard band
+static void count_guard_band(aleph_b200_handle* h, uint32_t n, const int32_t* status) {
+  h->stats.guard_band_shots += (uint32_t)status[2];
+  if (n > kExactCumulativeMaxN) h->stats.guard_band_inexact += (uint32_t)status[2];
+}
+
 int aleph_b200_sample(aleph_b200_handle* h, aleph_b200_state* st, uint32_t shots, int mode, const void* variates,
                       uint64_t* out) {
   if (!h || !st || (shots && (!variates || !out))) return ALEPH_B200_INVALID_ARGUMENT;
@@ -1404,6 +1440,7 @@ int aleph_b200_sample(aleph_b200_handle* h, aleph_b200_state* st, uint32_t shots
   CK(copy_async(h, status, dstatus, 16, cudaMemcpyDeviceToHost, h->stream), "status readback");
   CK(copy_async(h, out, dout, vb, cudaMemcpyDeviceToHost, h->stream), "sample readback");
   CK(cudaStreamSynchronize(h->stream), "stream synchronize");
+  if (mode == ALEPH_B200_SAMPLE_CUMULATIVE) count_guard_band(h, st->n, status);
   if (status[0]) {
     aleph_b200_error_info e{};
     e.status = status[0];
@@ -1442,23 +1479,15 @@ int aleph_b200_sample_seeded(aleph_b200_handle* h, aleph_b200_state* st, uint32_
 // loop, where the allocating path's scratch growth (cudaFree + cudaMalloc)
 // would synchronise the whole device and stall other streams.
 namespace {
-constexpr int kMaxFixedDevices = 64;
-std::mutex g_fixed_mu;
-void* g_fixed_base[kMaxFixedDevices] = {};
-
-// Address of this device's fixed buffer; the first call per device looks it
-// up (the device is current: bind() ran before).
+// Address of the current device's fixed buffer (bind() made the handle's
+// device current). Looked up on every call: the lookup is cheap once the
+// module is loaded (aleph_b200_create loads it), and a cached address would
+// go stale if the host program reset the device.
 int fixed_base(aleph_b200_handle* h, char** out) {
-  if (h->device < 0 || h->device >= kMaxFixedDevices)
-    return set_error(h, ALEPH_B200_INVALID_ARGUMENT, "device %d has no fixed sampling buffer", h->device);
-  std::lock_guard<std::mutex> lock(g_fixed_mu);
-  if (!g_fixed_base[h->device]) {
-    void* p = nullptr;
-    cudaError_t e = fixed_sample_scratch_address(&p);
-    if (e != cudaSuccess || !p) return cuda_fail(h, e != cudaSuccess ? e : cudaErrorInvalidSymbol, "fixed buffer address");
-    g_fixed_base[h->device] = p;
-  }
-  *out = (char*)g_fixed_base[h->device];
+  void* p = nullptr;
+  cudaError_t e = fixed_sample_scratch_address(&p);
+  if (e != cudaSuccess || !p) return cuda_fail(h, e != cudaSuccess ? e : cudaErrorInvalidSymbol, "fixed buffer address");
+  *out = (char*)p;
   return ALEPH_B200_OK;
 }
 }  // namespace
@@ -1491,6 +1520,7 @@ int aleph_b200_sample_cumulative_noalloc(aleph_b200_handle* h, aleph_b200_state*
   CK(copy_async(h, status, dstatus, 16, cudaMemcpyDeviceToHost, h->stream), "status readback");
   if (shots) CK(copy_async(h, out, dout, vb, cudaMemcpyDeviceToHost, h->stream), "sample readback");
   CK(cudaStreamSynchronize(h->stream), "stream synchronize");
+  count_guard_band(h, st->n, status);
   if (status[0]) {
     aleph_b200_error_info e{};
     e.status = status[0];
@@ -1736,6 +1766,29 @@ int aleph_b200_get_amplitudes(aleph_b200_handle* h, aleph_b200_state* st, double
   CK(copy_async(h, tmp.data(), st->amps, st->bytes, cudaMemcpyDeviceToHost, h->stream), "amplitude readback");
   CK(cudaStreamSynchronize(h->stream), "stream synchronize");
   for (uint64_t i = 0; i < 2 * len; ++i) out[i] = tmp[i];
+  return ALEPH_B200_OK;
+}
+
+int aleph_b200_get_amplitude_range(aleph_b200_handle* h, aleph_b200_state* st, uint64_t first, uint64_t count,
+                                   double* out) {
+  if (!h || !st || (count && !out)) return ALEPH_B200_INVALID_ARGUMENT;
+  const uint64_t len = 1ull << st->n;
+  if (first > len || count > len - first)
+    return set_error(h, ALEPH_B200_INVALID_ARGUMENT, "amplitude window [%llu, +%llu) outside 2^%u",
+                     (unsigned long long)first, (unsigned long long)count, st->n);
+  if (!count) return ALEPH_B200_OK;
+  if (int r = bind(h)) return r;
+  if (st->precision == ALEPH_B200_F64) {
+    CK(copy_async(h, out, (const char*)st->amps + first * 16, count * 16, cudaMemcpyDeviceToHost, h->stream),
+       "amplitude readback");
+    CK(cudaStreamSynchronize(h->stream), "stream synchronize");
+    return ALEPH_B200_OK;
+  }
+  std::vector<float> tmp(2 * count);
+  CK(copy_async(h, tmp.data(), (const char*)st->amps + first * 8, count * 8, cudaMemcpyDeviceToHost, h->stream),
+     "amplitude readback");
+  CK(cudaStreamSynchronize(h->stream), "stream synchronize");
+  for (uint64_t i = 0; i < 2 * count; ++i) out[i] = tmp[i];
   return ALEPH_B200_OK;
 }
 

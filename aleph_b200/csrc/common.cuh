@@ -124,6 +124,16 @@ __device__ __forceinline__ uint64_t insert_zero(uint64_t x, uint32_t pos) {
   return ((x >> pos) << (pos + 1)) | lo;
 }
 
+// Nanoseconds of the GPU's global timer.
+__device__ __forceinline__ uint64_t globaltimer_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+// Deadline of every bounded wait: a pipeline stage that has not completed
+// within this time is treated as stuck, and the kernel reports an error.
+constexpr uint64_t kWaitDeadlineNs = 1000000000ull;  // 1 s
+
 // ---- mbarriers and bulk-async copies (shared by the pipelined kernels) ------
 namespace async {
 __device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -145,11 +155,20 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// Bounded wait for the phase with the given parity: false on expiry.
-__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity, long long limit) {
-  for (long long i = 0; i < limit; ++i)
+// Wait for the phase with the given parity, bounded by kWaitDeadlineNs of
+// wall time (not by an iteration count: one try_wait may itself suspend the
+// thread for a while). Returns false on expiry, or once *abort_flag is set
+// by another role of the kernel (polled every 256 tries).
+__device__ __forceinline__ bool mbar_wait_deadline(uint32_t bar, uint32_t parity, volatile int* abort_flag) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = globaltimer_ns();
+  for (uint32_t i = 1;; ++i) {
     if (mbar_try_wait(bar, parity)) return true;
-  return false;
+    if ((i & 255) == 0) {
+      if (abort_flag && *abort_flag) return false;
+      if (globaltimer_ns() - t0 > kWaitDeadlineNs) return false;
+    }
+  }
 }
 // Non-multicast bulk copy global -> shared, completing on an mbarrier.
 __device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {

@@ -279,6 +279,9 @@ cudaError_t launch_qaoa_sweep(int precision, const aleph_b200_qaoa_set* sets, co
                               int grid, cudaStream_t s);
 
 // sampling (kernels_sample.cu)
+// CUMULATIVE: shots in the rounding guard band are re-resolved against the
+// exact sequential prefix sum up to this n; the count goes to status[2].
+constexpr uint32_t kExactCumulativeMaxN = 28;
 size_t sample_scratch_bytes(uint32_t n, int mode, uint32_t shots);
 cudaError_t launch_sample(const void* amps, int precision, uint32_t n, uint32_t shots, int mode, const void* variates_dev,
                           uint64_t* out_dev, void* scratch, size_t scratch_bytes, int32_t* status, int sm_count,
@@ -294,8 +297,11 @@ void build_block_image(const double* W, uint8_t* out);
 constexpr uint32_t kBlockImageBytes = 65536;
 
 // planner (planner.cpp)
+// tiled: the gate is one of a TiledBlock's gates, validated as the
+// reference's tiled executor does (fixed-size 2x2 / 4x4 matrix, no
+// unitarity check)
 int lower_gate(const aleph_b200_instr& g, uint32_t n, const double* pool, uint64_t pool_len, Lowered* out,
-               aleph_b200_error_info* err);
+               aleph_b200_error_info* err, bool tiled = false);
 int lower_diagonal_phase(const aleph_b200_phase_term* terms, uint64_t n_terms, const uint64_t* conds, uint64_t n_conds,
                          Lowered* out, aleph_b200_error_info* err);
 const char* gate_name(uint32_t kind);

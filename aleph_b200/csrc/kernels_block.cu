@@ -73,7 +73,6 @@ constexpr int MAX_RUNS = 128;                 // runs per tile (contiguous prefi
 constexpr int W_BYTES = 2 * 128 * 128 * 2;    // hi + lo images, 64 KiB
 constexpr uint32_t TMEM_COLS = 512;
 constexpr uint32_t TM_D = 0, TM_A = 256;      // accumulators / A operands (128 columns each)
-constexpr long long SPIN_LIMIT = 1ll << 26;   // bounded mbarrier waits
 constexpr int MAX_POST = 48;
 
 // shared-memory map (offsets from a 1024-byte aligned base)
@@ -108,13 +107,18 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// Bounded wait: false on expiry or when another role has aborted.
+// Bounded wait: false once about 1 s of wall time has passed
+// (kWaitDeadlineNs, %globaltimer) or when another role has aborted.
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag) {
-  for (long long i = 0; i < SPIN_LIMIT; ++i) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = globaltimer_ns();
+  for (uint32_t i = 1;; ++i) {
     if (mbar_try_wait(bar, parity)) return true;
-    if ((i & 1023) == 1023 && *abort_flag) return false;
+    if ((i & 255) == 0) {
+      if (*abort_flag) return false;
+      if (globaltimer_ns() - t0 > kWaitDeadlineNs) return false;
+    }
   }
-  return false;
 }
 __device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
   asm volatile(

@@ -25,7 +25,7 @@
 namespace ab {
 
 constexpr uint32_t CUM_BLOCK = 2048;  // amplitudes per level-1 CDF block
-constexpr uint32_t EXACT_MAX_N = 28;  // exact re-resolution of ambiguous shots up to this n
+constexpr uint32_t EXACT_MAX_N = kExactCumulativeMaxN;  // exact re-resolution of ambiguous shots up to this n
 
 template <typename Real>
 __device__ __forceinline__ double prob_exact(const V2<Real>* amps, uint64_t i) {
@@ -590,6 +590,8 @@ cudaError_t launch_sample(const void* amps, int precision, uint32_t n, uint32_t 
     else
       cum_draw_kernel<float><<<(shots + 127) / 128, 128, 0, st>>>((const float2*)amps, len, nb, c,
                                                                   (const double*)variates, shots, out, status);
+    // status[2]: the shots inside the guard band (re-resolved below when n <= EXACT_MAX_N)
+    cudaMemcpyAsync(status + 2, c.namb, 4, cudaMemcpyDeviceToDevice, st);
     if (n <= EXACT_MAX_N) {
       const unsigned eb = (shots + 127) / 128;
       if (f64) {

@@ -319,7 +319,7 @@ const char* gate_name(uint32_t kind) {
 }
 
 int lower_gate(const aleph_b200_instr& g, uint32_t n, const double* pool, uint64_t pool_len, Lowered* L,
-               aleph_b200_error_info* e) {
+               aleph_b200_error_info* e, bool tiled) {
   const int expected = arity(g);
   if (expected < 0) {
     set_kind(e, gate_name(g.kind));
@@ -352,6 +352,13 @@ int lower_gate(const aleph_b200_instr& g, uint32_t n, const double* pool, uint64
       }
     seen[ns++] = q;
     if (i >= g.num_qubits) ctrl |= 1ull << q;
+  }
+  if (tiled && g.kind == ALEPH_GATE_UNITARYKQ) {
+    // a gate of a TiledBlock goes through Gate::matrix() only
+    // (dispatch_tile_kernel, crates/aleph-sv/src/backend.rs:265-299), and a
+    // UnitaryKq has no fixed-size matrix there: UnsupportedGate
+    set_kind(e, gate_name(g.kind));
+    return fail(e, ALEPH_B200_UNSUPPORTED_GATE);
   }
   if (g.kind == ALEPH_GATE_UNITARYKQ) {
     // validate_unitary_kq, crates/aleph-sv/src/validation.rs:113-155
@@ -406,6 +413,16 @@ int lower_gate(const aleph_b200_instr& g, uint32_t n, const double* pool, uint64
   Cx flat[64];
   for (int i = 0; i < dim; ++i)
     for (int j = 0; j < dim; ++j) flat[i * dim + j] = m[i][j];
+  if (tiled) {
+    // TiledBlock gates: the tile kernels take 2x2 and 4x4 matrices; an 8x8
+    // is UnsupportedGate, and no unitarity check is made (backend.rs:265-299)
+    if (dim > 4) {
+      set_kind(e, gate_name(g.kind));
+      return fail(e, ALEPH_B200_UNSUPPORTED_GATE);
+    }
+    lower_matrix(flat, dim, g.qubits, ctrl, L);
+    return ALEPH_B200_OK;
+  }
   const double dev = unitarity_deviation(flat, dim);
   if (!std::isfinite(dev) || dev > kTol) {
     e->value = dev;

@@ -94,7 +94,7 @@ typedef enum aleph_b200_kind {
   /* non-gate instructions (crates/aleph-ir/src/instruction.rs:13-34) */
   ALEPH_INSTR_MEASURE = 100,        /* qubits[0] = qubit, aux = clbit           */
   ALEPH_INSTR_RESET = 101,          /* rejected: UnsupportedInstruction "reset" */
-  ALEPH_INSTR_BARRIER = 102,        /* no-op                                    */
+  ALEPH_INSTR_BARRIER = 102,        /* no-op; data_offset = mask of its qubits  */
   ALEPH_INSTR_DIAGONAL_PHASE = 103, /* terms [data_offset, data_offset+data_len) */
   ALEPH_INSTR_TILED_BLOCK = 104     /* aux = tile_bits; the next data_len records are its gates */
 } aleph_b200_kind;
@@ -268,15 +268,16 @@ int aleph_b200_sample_seeded(aleph_b200_handle* h, aleph_b200_state* st, uint32_
 
 /* CUMULATIVE sampling that allocates nothing. No counterpart in the reference.
  * Same kernels and results as aleph_b200_sample(..., ALEPH_B200_SAMPLE_CUMULATIVE,
- * ...), but all device scratch lives in one fixed 8 MiB buffer reserved when
- * the library's module loads on a device (no cudaMalloc / cudaFree), for
- * callers that cannot allocate at that point: state vectors that already fill
- * HBM, or latency-bound sampling loops where scratch growth would synchronise
- * the device.
+ * ...), but all device scratch lives in one fixed 8 MiB buffer per device (no
+ * cudaMalloc / cudaFree), for callers that cannot allocate at that point:
+ * state vectors that already fill HBM, or latency-bound sampling loops where
+ * scratch growth would synchronise the device.
+ *  - The buffer is reserved when the first handle on a device is created
+ *    (aleph_b200_create loads the module that holds it), before any state is
+ *    allocated; each call looks up its address with the handle's device
+ *    current, so a device reset by the host program is followed correctly.
  *  - Limit: the scratch of (n, shots) must fit the 8 MiB (n <= 30 fits up to
  *    65536 shots); larger requests return ALEPH_B200_INVALID_ARGUMENT.
- *  - The first call on each device looks up the buffer's address (with that
- *    device current) and should precede any stream capture.
  *  - The buffer is shared by all handles on a device: calls that overlap in
  *    time on one device (several host threads, or handles whose streams
  *    run concurrently) race on it; serialise them. Each call synchronises
@@ -311,6 +312,14 @@ int aleph_b200_probabilities(aleph_b200_handle* h, aleph_b200_state* st, const u
 /* ---- state access (RunResult.statevector(), crates/aleph-py/src/run.rs:71-101) ----
  * Interleaved (re, im) doubles, 2 * 2^n values; FP32 states are widened. */
 int aleph_b200_get_amplitudes(aleph_b200_handle* h, aleph_b200_state* st, double* out);
+/* A window of the state: amplitudes [first, first + count) as interleaved
+ * (re, im) doubles, for states too large to copy whole to the host (an n=33
+ * FP64 state is 128 GiB). The same values as the matching slice of
+ * aleph_b200_get_amplitudes (CudaSvState::amplitudes_vec,
+ * crates/aleph-cuda/src/sv/state.rs:106); a window outside 2^n amplitudes is
+ * ALEPH_B200_INVALID_ARGUMENT. */
+int aleph_b200_get_amplitude_range(aleph_b200_handle* h, aleph_b200_state* st, uint64_t first, uint64_t count,
+                                   double* out);
 int aleph_b200_set_amplitudes(aleph_b200_handle* h, aleph_b200_state* st, const double* in);
 /* FP64 sum of |a_i|^2 on the device. */
 int aleph_b200_norm_sqr(aleph_b200_handle* h, aleph_b200_state* st, double* out);
@@ -403,6 +412,13 @@ typedef struct aleph_b200_stats {
   double algorithmic_bytes;   /* sum of (amplitudes read + written) * bytes/amp     */
   uint64_t h2d_bytes;         /* bytes copied host -> device (plans, variates, ...) */
   uint64_t d2h_bytes;         /* bytes copied device -> host (results, status)      */
+  uint64_t guard_band_shots;  /* CUMULATIVE shots whose target fell within the
+                                 rounding guard band of a bin boundary of the
+                                 parallel prefix sums                              */
+  uint64_t guard_band_inexact;/* of those, shots on states above n = 28, which are
+                                 not re-resolved against the sequential sum: their
+                                 outcome may differ from the sequential CPU scan's
+                                 by one bin                                        */
 } aleph_b200_stats;
 int aleph_b200_get_stats(const aleph_b200_handle* h, aleph_b200_stats* out);
 int aleph_b200_reset_stats(aleph_b200_handle* h);

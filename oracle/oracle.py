@@ -50,6 +50,16 @@ def lib() -> ct.CDLL:
             "orc_norm_sqr": ([D, ct.c_uint32, D], ct.c_int),
             "orc_run_stream": ([D, ct.c_uint32, ct.POINTER(abi.Instr), ct.c_uint64, ct.POINTER(abi.Pools), D,
                                 ct.c_uint64, ct.POINTER(ct.c_uint8), ct.c_uint64, U64, U64], ct.c_int),
+            "orc_pipeline_describe": ([ct.c_uint32, ct.POINTER(abi.Instr), ct.c_uint64, ct.POINTER(abi.Pools),
+                                       ct.c_uint32, ct.c_uint32, U64], ct.c_int),
+            "orc_pipeline_run": ([D, ct.c_uint32, ct.POINTER(abi.Instr), ct.c_uint64, ct.POINTER(abi.Pools),
+                                  ct.c_uint32, ct.c_uint32, D, ct.c_uint64, D, U64], ct.c_int),
+            "orc_pipeline_plan": ([ct.c_uint32, ct.POINTER(abi.Instr), ct.c_uint64, ct.POINTER(abi.Pools),
+                                   ct.c_uint32, ct.c_uint32, ct.POINTER(ct.c_void_p)], ct.c_int),
+            "orc_pipeline_len": ([ct.c_void_p], ct.c_uint64),
+            "orc_pipeline_free": ([ct.c_void_p], None),
+            "orc_pipeline_exec": ([ct.c_void_p, D, ct.c_uint64, ct.c_uint64, ct.c_int, D, ct.c_uint64, U64, D],
+                                  ct.c_int),
         }
         for k, (a, r) in sig.items():
             f = getattr(L, k)
@@ -165,3 +175,74 @@ def gate_matrix(inst) -> np.ndarray:
     _check(lib().orc_gate_matrix(flat.instrs, flat.matrix_ptr, flat.matrix.size // 2, _dp(out), ct.byref(dim)))
     d = dim.value
     return (out[0:2 * d * d:2] + 1j * out[1:2 * d * d:2]).reshape(d, d)
+
+
+# ---- the reference's default optimised CPU path (sv_pipeline.cpp) ----------------
+PIPELINE_FIELDS = ("input", "after_cancel", "after_fuse1q", "after_fuse2q", "after_fusekq", "output",
+                   "tiled_blocks", "fused_kq", "relabeled")
+
+
+def describe_pipeline(n: int, instructions, tile_bits: int = 15, max_k: int = 4, flat=None) -> dict:
+    """Instruction counts after each pass of final_state_cpu_pipeline (host only)."""
+    flat = flat or flatten(instructions)
+    out = (ct.c_uint64 * 9)()
+    st = lib().orc_pipeline_describe(n, flat.instrs, flat.n, ct.byref(flat.pools), tile_bits, max_k, out)
+    if st != 0:
+        raise OracleError(st, abi.ErrorInfo())
+    return dict(zip(PIPELINE_FIELDS, (int(x) for x in out)))
+
+
+def run_pipeline(n: int, instructions, uniforms=None, state: np.ndarray | None = None, tile_bits: int = 15,
+                 max_k: int = 4, flat=None):
+    """run_optimized_cpu_final_state: the final-state CPU pass pipeline, then
+    the optimised circuit on the CPU sv kernels (crates/aleph-backend/src/lib.rs:308-318).
+    Returns (state, info) with planning / execution seconds and pass counts."""
+    flat = flat or flatten(instructions)
+    psi = zero_state(n) if state is None else np.array(state, dtype=np.complex128, copy=True)
+    u = np.ascontiguousarray(np.asarray(uniforms if uniforms is not None else [], dtype=np.float64))
+    secs = (ct.c_double * 2)()
+    counts = (ct.c_uint64 * 9)()
+    st = lib().orc_pipeline_run(_dp(psi), n, flat.instrs, flat.n, ct.byref(flat.pools), tile_bits, max_k,
+                                _dp(u) if u.size else None, u.size, secs, counts)
+    if st != 0:
+        info = abi.ErrorInfo()
+        lib().orc_last_error(ct.byref(info))
+        raise OracleError(st, info)
+    info = dict(zip(PIPELINE_FIELDS, (int(x) for x in counts)))
+    info["plan_s"], info["exec_s"] = secs[0], secs[1]
+    return psi, info
+
+
+class PlannedCircuit:
+    """A circuit planned once by the final-state CPU pipeline and executed in
+    slices (bench.py's reference arm times it a slice per step)."""
+
+    def __init__(self, n: int, instructions, tile_bits: int = 15, max_k: int = 4, flat=None):
+        self.n = n
+        self._flat = flat or flatten(instructions)
+        self._p = ct.c_void_p()
+        _check(lib().orc_pipeline_plan(n, self._flat.instrs, self._flat.n, ct.byref(self._flat.pools), tile_bits,
+                                       max_k, ct.byref(self._p)))
+
+    def __len__(self) -> int:
+        return int(lib().orc_pipeline_len(self._p))
+
+    def execute(self, psi: np.ndarray, i0: int = 0, i1: int | None = None, finish: bool = True) -> float:
+        """Runs planned instructions [i0, i1) on psi in place; returns seconds."""
+        secs = ct.c_double()
+        used = ct.c_uint64()
+        i1 = len(self) if i1 is None else i1
+        _check(lib().orc_pipeline_exec(self._p, _dp(psi), i0, i1, 1 if finish else 0, None, 0, ct.byref(used),
+                                       ct.byref(secs)))
+        return secs.value
+
+    def free(self):
+        if self._p:
+            lib().orc_pipeline_free(self._p)
+            self._p = ct.c_void_p()
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass

@@ -419,6 +419,11 @@ int check_qubits(const uint32_t* q, uint32_t k, uint32_t n) {
 
 }  // namespace
 
+namespace {
+int apply_gate_impl(double* amps_d, uint32_t n, const aleph_b200_instr* g, const double* pool, uint64_t pool_len,
+                    bool tiled);
+}
+
 extern "C" {
 
 // Reset the thread-local error before each call.
@@ -442,6 +447,25 @@ int orc_init(double* amps, uint32_t n) {
 // bounds and duplicates (qubits then controls), UnitaryKq validation, matrix
 // materialisation, unitarity check (deviation > 1e-10 rejects), dispatch.
 int orc_apply_gate(double* amps_d, uint32_t n, const aleph_b200_instr* g, const double* pool, uint64_t pool_len) {
+  return apply_gate_impl(amps_d, n, g, pool, pool_len, false);
+}
+
+// One gate of a TiledBlock: NaiveSvBackend::apply_tiled_block and
+// dispatch_tile_kernel (crates/aleph-sv/src/backend.rs:173-208,265-299) take
+// the gate's fixed-size matrix (Gate::matrix errors as for apply_gate;
+// UnitaryKq has none: UnsupportedGate), route 2x2 and 4x4 to the tile
+// kernels, reject 8x8 as UnsupportedGate, and make no unitarity check. The
+// tile-by-tile order gives the same amplitudes as applying the gates to the
+// whole state one after another (backend.rs:420-457), which is done here.
+int orc_apply_tiled_gate(double* amps_d, uint32_t n, const aleph_b200_instr* g, const double* pool,
+                         uint64_t pool_len) {
+  return apply_gate_impl(amps_d, n, g, pool, pool_len, true);
+}
+}  // extern "C"
+
+namespace {
+int apply_gate_impl(double* amps_d, uint32_t n, const aleph_b200_instr* g, const double* pool, uint64_t pool_len,
+                    bool tiled) {
   clear_err();
   C* amps = reinterpret_cast<C*>(amps_d);
   int expected = gate_arity(*g);
@@ -461,6 +485,10 @@ int orc_apply_gate(double* amps_d, uint32_t n, const aleph_b200_instr* g, const 
   for (uint32_t i = 0; i < g->num_qubits; ++i) all[na++] = g->qubits[i];
   for (uint32_t i = 0; i < g->num_controls; ++i) all[na++] = g->controls[i];
   if (int s = check_qubits(all, na, n)) return s;
+  if (tiled && g->kind == ALEPH_GATE_UNITARYKQ) {
+    set_kind(gate_name(g->kind));
+    return fail(ALEPH_B200_UNSUPPORTED_GATE);
+  }
   if (g->kind == ALEPH_GATE_UNITARYKQ) {
     uint32_t k = g->aux;
     if (!pool || g->data_offset + g->data_len > pool_len) return fail(ALEPH_B200_INVALID_ARGUMENT);
@@ -472,10 +500,16 @@ int orc_apply_gate(double* amps_d, uint32_t n, const aleph_b200_instr* g, const 
   C m[8][8];
   int dim = gate_matrix(*g, pool, pool_len, m);
   if (dim == 0) return g_err.status;
-  double dev = unitarity_deviation(m, dim);
-  if (!std::isfinite(dev) || dev > kAmplitudeTol) {
-    g_err.info.value = dev;
-    return fail(ALEPH_B200_NON_UNITARY_MATRIX);
+  if (tiled && dim > 4) {
+    set_kind(gate_name(g->kind));
+    return fail(ALEPH_B200_UNSUPPORTED_GATE);
+  }
+  if (!tiled) {
+    double dev = unitarity_deviation(m, dim);
+    if (!std::isfinite(dev) || dev > kAmplitudeTol) {
+      g_err.info.value = dev;
+      return fail(ALEPH_B200_NON_UNITARY_MATRIX);
+    }
   }
   C flat[64];
   for (int i = 0; i < dim; ++i)
@@ -484,6 +518,9 @@ int orc_apply_gate(double* amps_d, uint32_t n, const aleph_b200_instr* g, const 
   apply_dense(amps, n, g->qubits, k, flat, g->controls, g->num_controls);
   return ALEPH_B200_OK;
 }
+}  // namespace
+
+extern "C" {
 
 // Gate matrix (for tests of the host-side matrix builder). Writes dim*dim complex.
 int orc_gate_matrix(const aleph_b200_instr* g, const double* pool, uint64_t pool_len, double* out, int* dim_out) {
@@ -773,20 +810,27 @@ int orc_norm_sqr(const double* amps_d, uint32_t n, double* out) {
 
 // run_with_outcomes, crates/aleph-backend/src/lib.rs:211-245, over the flat
 // instruction stream. Measurements take one uniform from `uniforms` each time
-// both branches are non-degenerate. TILED_BLOCK records are replayed gate by
-// gate (Backend::apply_tiled_block default, lib.rs:135-146; the tiled CPU
-// kernel is bit-identical to it, backend.rs:173-208).
+// both branches are non-degenerate. The gates of a TILED_BLOCK record follow
+// it and go through orc_apply_tiled_gate (NaiveSvBackend::apply_tiled_block,
+// crates/aleph-sv/src/backend.rs:173-299).
 int orc_run_stream(double* amps, uint32_t n, const aleph_b200_instr* instrs, uint64_t count,
                    const aleph_b200_pools* pools, const double* uniforms, uint64_t n_uniforms, uint8_t* outcomes,
                    uint64_t outcomes_cap, uint64_t* n_outcomes, uint64_t* failed_at) {
   clear_err();
-  uint64_t used = 0, nout = 0;
+  uint64_t used = 0, nout = 0, tiled_left = 0;
   *failed_at = UINT64_MAX;
   for (uint64_t i = 0; i < count; ++i) {
     const aleph_b200_instr& g = instrs[i];
     int s = ALEPH_B200_OK;
-    if (g.kind < 28) {
-      s = orc_apply_gate(amps, n, &g, pools ? pools->matrix_pool : nullptr, pools ? pools->matrix_pool_len : 0);
+    const bool tiled = tiled_left > 0;
+    if (tiled) --tiled_left;
+    if (tiled && g.kind >= 28) {
+      clear_err();
+      set_kind("tiled block member");
+      s = fail(ALEPH_B200_INVALID_ARGUMENT);
+    } else if (g.kind < 28) {
+      s = apply_gate_impl(amps, n, &g, pools ? pools->matrix_pool : nullptr, pools ? pools->matrix_pool_len : 0,
+                          tiled);
     } else if (g.kind == ALEPH_INSTR_MEASURE) {
       if (g.num_qubits != 1) {
         s = fail(ALEPH_B200_INVALID_ARGUMENT);
@@ -810,8 +854,15 @@ int orc_run_stream(double* amps, uint32_t n, const aleph_b200_instr* instrs, uin
       clear_err();
       set_kind("reset");
       s = fail(ALEPH_B200_UNSUPPORTED_INSTRUCTION);
-    } else if (g.kind == ALEPH_INSTR_BARRIER || g.kind == ALEPH_INSTR_TILED_BLOCK) {
+    } else if (g.kind == ALEPH_INSTR_BARRIER) {
       s = ALEPH_B200_OK;
+    } else if (g.kind == ALEPH_INSTR_TILED_BLOCK) {
+      if (g.data_len > count - i - 1) {
+        clear_err();
+        set_kind("tiled block length");
+        s = fail(ALEPH_B200_INVALID_ARGUMENT);
+      }
+      tiled_left = g.data_len;
     } else if (g.kind == ALEPH_INSTR_DIAGONAL_PHASE) {
       if (!pools || g.data_offset + g.data_len > pools->n_terms) s = fail(ALEPH_B200_INVALID_ARGUMENT);
       else

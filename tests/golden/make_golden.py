@@ -8,7 +8,7 @@ reference's parser lowers (crates/aleph-parser/src/lower.rs:255-283) and
 stored as a list of operations beside the expected amplitudes, so the tests
 need neither the reference tree nor a QASM parser at run time.
 
-Usage:  python tests/golden/make_golden.py [/path/to/reference]
+Usage:  python tests/golden/make_golden.py /path/to/reference
 """
 from __future__ import annotations
 
@@ -91,4 +91,6 @@ def main(ref: Path) -> None:
 
 
 if __name__ == "__main__":
-    main(Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference"))
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py <path of the aleph reference checkout>")
+    main(Path(sys.argv[1]))

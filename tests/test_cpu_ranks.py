@@ -48,7 +48,7 @@ def test_ranks_barrier_and_max_over_ranks(tmp_path):
 
 def test_reference_arm_prints_one_line_from_rank_zero():
     res = torchrun(["bench.py", "--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "3",
-                    "--ref-sample-n", "14"])
+                    "--ref-n", "14"])
     assert res.returncode == 0, res.stderr[-2000:]
     lines = [l for l in res.stdout.splitlines() if l.startswith("{")]
     assert len(lines) == 1

@@ -14,7 +14,7 @@ from aleph_b200 import circuit as C
 from aleph_b200 import workloads
 from aleph_b200.backend import B200SvBackend
 from oracle import oracle
-from tests.test_gpu_parity import random_circuit
+from tests.circuit_gen import random_circuit
 
 pytestmark = pytest.mark.gpu
 

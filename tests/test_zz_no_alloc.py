@@ -25,16 +25,27 @@ def fixed_sample(be, st, variates):
     return status, out[: v.size]
 
 
+def device_free_bytes():
+    import torch
+
+    free, _ = torch.cuda.mem_get_info(0)
+    return free
+
+
 @pytest.mark.parametrize("precision,n,shots", [("f64", 20, 4096), ("f32", 27, 2048)])
 def test_fixed_buffer_sampling_matches_allocating_entry_point(precision, n, shots):
-    be = B200SvBackend(seed=0, precision=precision)
+    be = B200SvBackend(seed=0, precision=precision)  # a fresh handle: the fixed buffer is reserved here
     st = run(be, workloads.brickwall(n, 3, seed=40 + n))
     u = np.random.default_rng(n).random(shots)
     want = be.sample(st, shots, variates=u, mode="cumulative")
+    be.synchronize()
+    free_before = device_free_bytes()
     for _ in range(2):  # two calls in a row reuse the same buffer
         status, got = fixed_sample(be, st, u)
         assert status == abi.OK
         assert np.array_equal(got, want)
+    # nothing was allocated on the device by the two calls
+    assert device_free_bytes() == free_before
 
 
 def test_fixed_buffer_rejects_requests_over_its_size():
