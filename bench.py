@@ -405,13 +405,18 @@ def learned_choice(be, n, flat, precision):
         model.free()
 
 
-def qaoa_sweep_bench(dev: int, sets: int, loop_sample: int, seed: int) -> dict:
+def qaoa_sweep_bench(dev: int, sets: int, loop_sample: int, seed: int, ranks: "Ranks") -> dict:
     """Batched QAOA Max-Cut sweep: `sets` parameter sets, n uniform in 12..24,
     random 3-regular graphs (odd n: random graphs with 3n/2 edges), p = 4,
-    angles uniform in [0, pi]; FP32 and FP64 states, <C> in FP64. Compared with
-    a per-circuit launch loop through the engine's gate-stream path."""
+    angles uniform in [0, pi]; FP32 and FP64 states, <C> in FP64. With N
+    ranks the sets are split into contiguous ranges balanced by sum(2^n), each
+    rank runs its range as one persistent launch on its GPU and the <C>
+    values are all-gathered (aleph_b200/sweep.py); the time is the max over
+    ranks. Rank 0 also times a per-circuit launch loop through the engine's
+    gate-stream path."""
     from aleph_b200 import workloads
     from aleph_b200.backend import B200SvBackend
+    from aleph_b200.sweep import partition_by_work, sharded_sweep
 
     rng = np.random.default_rng(seed)
     graphs = []
@@ -427,18 +432,24 @@ def qaoa_sweep_bench(dev: int, sets: int, loop_sample: int, seed: int) -> dict:
             graphs.append((n, sorted(e)))
     gam = rng.uniform(0, np.pi, (sets, 4))
     bet = rng.uniform(0, np.pi, (sets, 4))
-    out = {"sets": sets, "n_range": [12, 24], "p": 4}
+    out = {"sets": sets, "n_range": [12, 24], "p": 4, "ranks": ranks.world,
+           "partition": partition_by_work([n for n, _ in graphs], ranks.world)}
     vals = {}
     for prec in ("f32", "f64"):
         be = B200SvBackend(seed=0, device=dev, precision=prec)
-        be.qaoa_sweep(graphs, gam, bet)  # capture + warm-up
+
+        def sweep():
+            return sharded_sweep(graphs, gam, bet, be.qaoa_sweep, ranks.rank, ranks.world)
+
+        sweep()  # capture + warm-up
         ts = []
         for _ in range(3):
+            ranks.barrier()
             t0 = time.perf_counter()
-            vals[prec] = be.qaoa_sweep(graphs, gam, bet)
-            ts.append(time.perf_counter() - t0)
+            vals[prec] = sweep()
+            ts.append(ranks.max(time.perf_counter() - t0))
         out[f"{prec}_circuits_per_s"] = round(sets / min(ts), 1)
-        if prec == "f32":
+        if prec == "f32" and ranks.rank == 0:
             # one untimed pass over the sample first: first-call costs (kernel
             # loading, a state buffer of each new size, scratch growth) are
             # not per-circuit costs
@@ -473,7 +484,8 @@ def qaoa_sweep_bench(dev: int, sets: int, loop_sample: int, seed: int) -> dict:
             out["per_circuit_loop_term_by_term_circuits_per_s"] = round(1.0 / best[False], 1)
             out["per_circuit_loop_sample"] = loop_sample
         be.close()
-    out["sweep_speedup_f32"] = round(out["f32_circuits_per_s"] / out["per_circuit_loop_circuits_per_s"], 1)
+    if ranks.rank == 0:
+        out["sweep_speedup_f32"] = round(out["f32_circuits_per_s"] / out["per_circuit_loop_circuits_per_s"], 1)
     out["max_abs_c_f32_vs_f64"] = float(np.abs(vals["f32"] - vals["f64"]).max())
     return out
 
@@ -693,8 +705,8 @@ def run_engine(args, ranks: Ranks):
     oracle_psi = None
 
     qaoa = None
-    if args.qaoa_sets and ranks.rank == 0:
-        qaoa = qaoa_sweep_bench(dev, args.qaoa_sets, 32, args.seed)
+    if args.qaoa_sets:  # every rank runs its share of the sets
+        qaoa = qaoa_sweep_bench(dev, args.qaoa_sets, 32, args.seed, ranks)
     small = None
     if not args.skip_small and ranks.rank == 0:
         small = small_configs_bench(dev, args.seed, greedy=args.greedy)
