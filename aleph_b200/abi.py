@@ -214,6 +214,7 @@ _SIGNATURES = {
     "aleph_b200_probabilities": ([_P, _P, ct.POINTER(ct.c_uint32), ct.c_uint32, ct.POINTER(ct.c_double)], ct.c_int),
     "aleph_b200_get_amplitudes": ([_P, _P, ct.POINTER(ct.c_double)], ct.c_int),
     "aleph_b200_get_amplitude_range": ([_P, _P, ct.c_uint64, ct.c_uint64, ct.POINTER(ct.c_double)], ct.c_int),
+    "aleph_b200_fp64_rate": ([_P, ct.POINTER(ct.c_double)], ct.c_int),
     "aleph_b200_set_amplitudes": ([_P, _P, ct.POINTER(ct.c_double)], ct.c_int),
     "aleph_b200_norm_sqr": ([_P, _P, ct.POINTER(ct.c_double)], ct.c_int),
     "aleph_b200_synchronize": ([_P], ct.c_int),

@@ -251,6 +251,12 @@ class B200SvBackend:
                                                        out.ctypes.data_as(ct.POINTER(ct.c_double))))
         return out[0::2] + 1j * out[1::2]
 
+    def fp64_rate(self) -> float:
+        """The FP64 FMA rate of the device's CUDA cores, TFLOP/s, measured now."""
+        v = ct.c_double()
+        self._check(self.lib.aleph_b200_fp64_rate(self.handle, ct.byref(v)))
+        return v.value
+
     def amplitude_range(self, state: State, first: int, count: int) -> np.ndarray:
         """Amplitudes [first, first + count) of a state of any size."""
         out = np.zeros(2 * max(1, count), dtype=np.float64)

@@ -1769,6 +1769,32 @@ int aleph_b200_get_amplitudes(aleph_b200_handle* h, aleph_b200_state* st, double
   return ALEPH_B200_OK;
 }
 
+int aleph_b200_fp64_rate(aleph_b200_handle* h, double* tflops) {
+  if (!h || !tflops) return ALEPH_B200_INVALID_ARGUMENT;
+  if (int r = bind(h)) return r;
+  const uint32_t blocks = (uint32_t)h->sm_count * 8, iters = 20000;
+  if (int r = ensure(h, h->reduce, (size_t)blocks * 256 * 8 + 256)) return r;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  CK(cudaEventCreate(&e0), "event");
+  cudaError_t ce = cudaEventCreate(&e1);
+  float best = 0.f;
+  for (int k = 0; k < 4 && ce == cudaSuccess; ++k) {  // one warm-up launch, then three timed
+    ce = cudaEventRecord(e0, h->stream);
+    if (ce == cudaSuccess) ce = launch_dfma_peak((double*)h->reduce.ptr, blocks, iters, h->stream);
+    if (ce == cudaSuccess) ce = cudaEventRecord(e1, h->stream);
+    if (ce == cudaSuccess) ce = cudaEventSynchronize(e1);
+    float ms = 0.f;
+    if (ce == cudaSuccess) ce = cudaEventElapsedTime(&ms, e0, e1);
+    h->stats.kernel_launches++;
+    if (k > 0 && ce == cudaSuccess && (best == 0.f || ms < best)) best = ms;
+  }
+  cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  if (ce != cudaSuccess) return cuda_fail(h, ce, "fp64 rate");
+  *tflops = 2.0 * dfma_per_launch(blocks, iters) / (best * 1e-3) / 1e12;
+  return ALEPH_B200_OK;
+}
+
 int aleph_b200_get_amplitude_range(aleph_b200_handle* h, aleph_b200_state* st, uint64_t first, uint64_t count,
                                    double* out) {
   if (!h || !st || (count && !out)) return ALEPH_B200_INVALID_ARGUMENT;

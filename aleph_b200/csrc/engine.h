@@ -278,6 +278,10 @@ cudaError_t launch_qaoa_sweep(int precision, const aleph_b200_qaoa_set* sets, co
                               void* scratch, uint8_t* cuts, uint64_t slice_amps, uint32_t n_sets, uint32_t p,
                               int grid, cudaStream_t s);
 
+// FP64 issue rate (kernels_peak.cu): DFMA chains only, no memory traffic
+cudaError_t launch_dfma_peak(double* out, uint32_t blocks, uint32_t iters, cudaStream_t s);
+double dfma_per_launch(uint32_t blocks, uint32_t iters);
+
 // sampling (kernels_sample.cu)
 // CUMULATIVE: shots in the rounding guard band are re-resolved against the
 // exact sequential prefix sum up to this n; the count goes to status[2].

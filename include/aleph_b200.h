@@ -402,6 +402,13 @@ int aleph_b200_mlp_gradients(aleph_b200_handle* h, aleph_b200_mlp* m, const floa
 int aleph_b200_mlp_train(aleph_b200_handle* h, aleph_b200_mlp* m, const float* X, const float* y, uint32_t n,
                          uint32_t epochs, uint32_t batch, float lr, uint64_t seed, float* final_loss);
 
+/* ---- measured FP64 rate (no counterpart in the reference) ----
+ * The double-precision FMA rate this device's CUDA cores sustain, in TFLOP/s
+ * (2 flops per FMA), measured now by a compute-only kernel on the handle's
+ * stream (best of three ~50 ms launches, CUDA events). It is the roofline of
+ * the plain FP64 tile passes, which become FMA-bound when many gates fuse. */
+int aleph_b200_fp64_rate(aleph_b200_handle* h, double* tflops);
+
 /* ---- launch statistics (execution_counters, crates/aleph-cuda/src/execution.rs:145-165) ---- */
 typedef struct aleph_b200_stats {
   uint64_t kernel_launches;   /* engine kernels launched by this handle            */

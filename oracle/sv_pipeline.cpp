@@ -53,14 +53,13 @@ namespace {
 
 using C = std::complex<double>;
 
+// Read on every parallel region, so a caller can time one run on one core
+// and the next on all of them.
 int threads() {
-  static int t = [] {
-    const char* e = std::getenv("ORACLE_THREADS");
-    int v = e ? std::atoi(e) : 0;
-    if (v <= 0) v = (int)std::thread::hardware_concurrency();
-    return v <= 0 ? 1 : v;
-  }();
-  return t;
+  const char* e = std::getenv("ORACLE_THREADS");
+  int v = e ? std::atoi(e) : 0;
+  if (v <= 0) v = (int)std::thread::hardware_concurrency();
+  return v <= 0 ? 1 : v;
 }
 
 // ---- instructions ----------------------------------------------------------
