@@ -72,7 +72,10 @@ def test_two_ranks_gather_the_single_rank_vector(tmp_path):
     script.write_text(SCRIPT.format(root=str(ROOT)))
     res = torchrun([str(script)])
     assert res.returncode == 0, res.stderr[-2000:]
-    lines = [json.loads(m) for m in re.findall(r"\{\"rank\"[^\n]*\}", res.stdout)]
+    # the ranks share one stdout, so two lines can arrive run together: decode
+    # each object from where it starts
+    dec = json.JSONDecoder()
+    lines = [dec.raw_decode(res.stdout, m.start())[0] for m in re.finditer(r"\{\"rank\"", res.stdout)]
     assert sorted(l["rank"] for l in lines) == [0, 1]
     for l in lines:
         assert l["full"] == l["alone"]  # identical doubles: same evaluation, gathered
