@@ -490,6 +490,67 @@ def qaoa_sweep_bench(dev: int, sets: int, loop_sample: int, seed: int, ranks: "R
     return out
 
 
+def reference_gpu_bench(dev: int, seed: int, depth: int, reps: int = 2) -> dict:
+    """The reference's own GPU path on this GPU beside the engine, on the
+    depth-`depth` brickwall at the reference's CUDA qubit caps (FP64 n=30,
+    crates/aleph-cuda/src/sv/state.rs:41; FP32 n=31, fp32.rs:48). The reference
+    arm is its CUDA kernels compiled from its sources (oracle/_ref), launched
+    in its run_layered order on the stream its CUDA pass list plans
+    (oracle/ref_gpu.cpp; held to the oracle by tests/test_gpu_refgpu.py).
+    Each side: best of `reps` runs from |0...0>, device time by events."""
+    import torch
+
+    from aleph_b200 import workloads
+    from aleph_b200.backend import B200SvBackend
+    from aleph_b200.circuit import flatten
+    from oracle import oracle
+
+    if not oracle.reference_gpu_available():
+        return {"unavailable": "reference kernels not built (oracle/_ref: make -C oracle ref)"}
+    out = {"workload": f"random brickwall depth {depth}, seed {seed}, |0...0> start",
+           "reference": "the reference's CUDA kernels (kernels.cu, diag.cu, kernels_f32.cu) compiled for sm_100a; "
+                        "CUDA pass list CancelInversePairs, FuseDiagonalRuns, Fuse1qRuns, Fuse2q, FuseKq(3); "
+                        "run_layered dispatch (apply_1q_multi batches of 3, apply_phase_poly, apply_kq_tiled)"}
+
+    def engine_ms(n, flat, precision):
+        be = B200SvBackend(seed=seed, device=dev, precision=precision)
+        stream = torch.cuda.ExternalStream(be.stream_ptr())
+        plan = be.compile(n, flat)
+        st = be.allocate(n)
+        be.reset_state(st)
+        plan.execute(st)
+        ms = []
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            be.reset_state(st)
+            plan.execute(st)
+            e1.record(stream)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        plan.free()
+        st.free()
+        be.close()
+        return min(ms)
+
+    for key, n, f32, forms in (("fp64_n30", 30, False, ("f64", "tc32")), ("fp32_n31", 31, True, ("f32", "tc32"))):
+        c = workloads.brickwall(n, depth, seed=seed)
+        plan = oracle.PlannedCircuit(n, c.instructions, max_k=3, gpu=True)
+        ref_ms, launches, _ = oracle.run_reference_gpu(plan, f32=f32, repeats=reps)
+        counts = plan.counts()
+        plan.free()
+        torch.cuda.synchronize()
+        row = {"n": n, "reference_ms": round(float(ref_ms.min()), 2), "reference_launches": launches,
+               "reference_instructions": counts["output"], "reference_diagonal_phases": counts["tiled_blocks"]}
+        flat = flatten(c.instructions)
+        for prec in forms:
+            ms = engine_ms(n, flat, prec)
+            row[f"engine_{prec}_ms"] = round(ms, 2)
+            row[f"speedup_{prec}"] = round(float(ref_ms.min()) / ms, 2)
+        out[key] = row
+    return out
+
+
 def out_of_core_bench(dev: int, seed: int, n: int = 28, depth: int = 4, tile_qubits: int = 20,
                       local_qubits: int = 26) -> dict:
     """The out-of-core path (aleph_b200_paged_run): an FP64 brickwall whose
@@ -713,6 +774,9 @@ def run_engine(args, ranks: Ranks):
     paged = None
     if not args.skip_paged and ranks.rank == 0:
         paged = out_of_core_bench(dev, args.seed)
+    refgpu = None
+    if not args.skip_refgpu and ranks.rank == 0:
+        refgpu = reference_gpu_bench(dev, args.seed, depth)
 
     if ranks.rank == 0:
         line = {
@@ -725,7 +789,7 @@ def run_engine(args, ranks: Ranks):
             "clocks": clk, "e2e": e2e, "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu,
             "kernels": table, "fp64_plain": fp64, "fidelity": fid, "final_norm_sqr": norm,
             "plan_choice": None if choice is None else dict(choice.__dict__, source="learned cost model"),
-            "qaoa_sweep": qaoa, "fp64_configs": small, "out_of_core": paged,
+            "qaoa_sweep": qaoa, "fp64_configs": small, "out_of_core": paged, "reference_gpu": refgpu,
         }
         print(json.dumps(line), flush=True)
     ranks.close()
@@ -764,6 +828,8 @@ def main(argv=None):
     ap.add_argument("--greedy", action="store_true", help="the greedy plan configuration, no cost model")
     ap.add_argument("--skip-small", action="store_true", help="skip the n=20 brickwall / n=30 QFT FP64 checks")
     ap.add_argument("--skip-paged", action="store_true", help="skip the out-of-core (host-paged) run")
+    ap.add_argument("--skip-refgpu", action="store_true",
+                    help="skip the reference's own GPU kernels timed beside the engine (FP64 n=30, FP32 n=31)")
     args = ap.parse_args(argv)
     args.warmup = max(3, args.warmup)  # at least 3 untimed warm-up steps
     ranks = Ranks()

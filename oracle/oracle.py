@@ -60,6 +60,15 @@ def lib() -> ct.CDLL:
             "orc_pipeline_free": ([ct.c_void_p], None),
             "orc_pipeline_exec": ([ct.c_void_p, D, ct.c_uint64, ct.c_uint64, ct.c_int, D, ct.c_uint64, U64, D],
                                   ct.c_int),
+            "orc_gpu_pipeline_plan": ([ct.c_uint32, ct.POINTER(abi.Instr), ct.c_uint64, ct.POINTER(abi.Pools),
+                                       ct.c_uint32, ct.POINTER(ct.c_void_p)], ct.c_int),
+            "orc_pipeline_records": ([ct.c_void_p, ct.POINTER(ct.POINTER(abi.Instr)), U64, ct.POINTER(abi.Pools)],
+                                     ct.c_int),
+            "orc_pipeline_counts": ([ct.c_void_p, U64], None),
+            "orc_refgpu_error": ([], ct.c_char_p),
+            "orc_refgpu_load": ([ct.c_char_p], ct.c_int),
+            "orc_refgpu_run": ([ct.c_uint32, ct.c_int, ct.POINTER(abi.Instr), ct.c_uint64, ct.POINTER(abi.Pools),
+                                ct.c_int, D, U64, D], ct.c_int),
         }
         for k, (a, r) in sig.items():
             f = getattr(L, k)
@@ -215,14 +224,36 @@ def run_pipeline(n: int, instructions, uniforms=None, state: np.ndarray | None =
 
 class PlannedCircuit:
     """A circuit planned once by the final-state CPU pipeline and executed in
-    slices (bench.py's reference arm times it a slice per step)."""
+    slices (bench.py's reference arm times it a slice per step). With
+    ``gpu=True`` the plan is the reference's CUDA pass list instead
+    (fuse_full_state, crates/aleph-cuda/src/fusion.rs:137-152: CancelInversePairs,
+    FuseDiagonalRuns, Fuse1qRuns, Fuse2q, FuseKq width 3), which runs here on
+    the CPU kernels or on the reference's own GPU kernels (``run_reference_gpu``)."""
 
-    def __init__(self, n: int, instructions, tile_bits: int = 15, max_k: int = 4, flat=None):
+    def __init__(self, n: int, instructions, tile_bits: int = 15, max_k: int = 4, flat=None, gpu: bool = False):
         self.n = n
         self._flat = flat or flatten(instructions)
         self._p = ct.c_void_p()
-        _check(lib().orc_pipeline_plan(n, self._flat.instrs, self._flat.n, ct.byref(self._flat.pools), tile_bits,
-                                       max_k, ct.byref(self._p)))
+        if gpu:
+            _check(lib().orc_gpu_pipeline_plan(n, self._flat.instrs, self._flat.n, ct.byref(self._flat.pools),
+                                               max_k, ct.byref(self._p)))
+        else:
+            _check(lib().orc_pipeline_plan(n, self._flat.instrs, self._flat.n, ct.byref(self._flat.pools),
+                                           tile_bits, max_k, ct.byref(self._p)))
+
+    def counts(self) -> dict:
+        """Pass counts; for a GPU plan `tiled_blocks` counts DiagonalPhase records."""
+        out = (ct.c_uint64 * 9)()
+        lib().orc_pipeline_counts(self._p, out)
+        return dict(zip(PIPELINE_FIELDS, (int(x) for x in out)))
+
+    def records(self):
+        """The planned instructions as flat records: (instr array, count, pools)."""
+        ptr = ct.POINTER(abi.Instr)()
+        cnt = ct.c_uint64()
+        pools = abi.Pools()
+        _check(lib().orc_pipeline_records(self._p, ct.byref(ptr), ct.byref(cnt), ct.byref(pools)))
+        return ptr, cnt.value, pools
 
     def __len__(self) -> int:
         return int(lib().orc_pipeline_len(self._p))
@@ -246,3 +277,29 @@ class PlannedCircuit:
             self.free()
         except Exception:
             pass
+
+
+# ---- the reference's own GPU kernels (ref_gpu.cpp; bench and tests only) ------------------
+REF_DIR = HERE / "_ref"
+
+
+def reference_gpu_available() -> bool:
+    return all((REF_DIR / f).exists() for f in ("sv_kernels.cubin", "sv_diag.cubin", "sv_kernels_f32.cubin"))
+
+
+def run_reference_gpu(plan: PlannedCircuit, f32: bool = False, repeats: int = 1, state: bool = False):
+    """Runs a GPU plan (``PlannedCircuit(..., gpu=True)``) on the reference's
+    CUDA kernels on device 0, from |0...0>, `repeats` times. Returns
+    (ms per run, launches per run, final state as complex128 or None)."""
+    L = lib()
+    if L.orc_refgpu_load(str(REF_DIR).encode()) != 0:
+        raise RuntimeError("reference GPU kernels: " + L.orc_refgpu_error().decode())
+    ptr, cnt, pools = plan.records()
+    ms = np.zeros(max(1, repeats), dtype=np.float64)
+    launches = ct.c_uint64()
+    psi = np.zeros(1 << plan.n, dtype=np.complex128) if state else None
+    rc = L.orc_refgpu_run(plan.n, 1 if f32 else 0, ptr, cnt, ct.byref(pools), repeats, _dp(ms), ct.byref(launches),
+                          _dp(psi) if state else None)
+    if rc != 0:
+        raise RuntimeError("reference GPU run: " + L.orc_refgpu_error().decode())
+    return ms, int(launches.value), psi

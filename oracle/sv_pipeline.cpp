@@ -712,6 +712,166 @@ void fuse_kq(std::vector<PInst>& v, uint32_t n, uint32_t max_qubits) {
   v = std::move(out);
 }
 
+// ---- FuseDiagonalRuns (crates/aleph-ir/src/passes/fuse_diagonal.rs) ----------------
+// GF(2) bit-permutation tracker (Perm, fuse_diagonal.rs:205-246): row[i] is the
+// mask whose parity with the run-start basis gives current bit i.
+struct GfPerm {
+  std::vector<uint64_t> row;
+  explicit GfPerm(uint32_t n) : row(n) {
+    for (uint32_t i = 0; i < n; ++i) row[i] = 1ull << i;
+  }
+  void cx(uint32_t c, uint32_t t) { row[t] ^= row[c]; }
+  uint64_t image(uint32_t b) const { return row[b]; }
+  uint64_t image_of_mask(uint64_t m) const {
+    uint64_t o = 0;
+    for (; m; m &= m - 1) o ^= row[__builtin_ctzll(m)];
+    return o;
+  }
+  bool identity() const {
+    for (size_t i = 0; i < row.size(); ++i)
+      if (row[i] != 1ull << i) return false;
+    return true;
+  }
+};
+
+constexpr double kPhaseEps = 1e-12;  // PHASE_EPS (fuse_diagonal.rs:249)
+
+double rem_2pi(double a) {  // f64::rem_euclid(2 pi)
+  const double tp = 2.0 * M_PI;
+  const double r = std::fmod(a, tp);
+  return r < 0 ? r + tp : r;
+}
+
+struct DTerm {
+  std::vector<uint64_t> conds;
+  double angle;
+};
+
+// diagonal_to_terms (fuse_diagonal.rs:266-310): the phase function of a
+// diagonal gate as a multilinear polynomial over its targets (Moebius
+// inversion), each monomial's conds mapped through the tracker; external
+// controls condition every term.
+bool diagonal_to_terms(const PGate& g, const GfPerm& perm, std::vector<DTerm>* out) {
+  if (!is_diagonal(g)) return false;
+  C m[64];
+  const int dim = matrix(g, m);
+  if (!dim) return false;
+  const uint32_t k = (uint32_t)g.q.size();
+  auto f = [&](uint32_t pattern) {
+    uint32_t r = 0;
+    for (uint32_t p = 0; p < k; ++p)
+      if ((pattern >> p) & 1) r |= 1u << (k - 1 - p);
+    return std::arg(m[r * dim + r]);
+  };
+  for (uint32_t s = 0; s < (1u << k); ++s) {
+    double alpha = 0.0;
+    for (uint32_t t = s;; t = (t - 1) & s) {
+      alpha += ((__builtin_popcount(s ^ t) & 1) ? -1.0 : 1.0) * f(t);
+      if (t == 0) break;
+    }
+    const double a = rem_2pi(alpha);
+    if (a < kPhaseEps || 2.0 * M_PI - a < kPhaseEps) continue;
+    DTerm term;
+    for (uint32_t p = 0; p < k; ++p)
+      if ((s >> p) & 1) term.conds.push_back(perm.image(g.q[p]));
+    for (uint32_t c : g.c) term.conds.push_back(perm.image(c));
+    term.angle = alpha;
+    out->push_back(std::move(term));
+  }
+  return true;
+}
+
+bool diag_run_member(const PInst& in) {  // is_run_member (fuse_diagonal.rs:72-80)
+  if (in.t == IK::Diag) return true;
+  return in.t == IK::Gate && (is_diagonal(in.g) || (in.g.kind == ALEPH_GATE_CNOT && in.g.c.empty()));
+}
+
+// fuse_run (fuse_diagonal.rs:86-157) and canonicalize (:164-190): one
+// DiagonalPhase for the run, or false to re-emit the run verbatim.
+bool fuse_diag_run(const std::vector<PInst>& v, size_t i0, size_t i1, uint32_t n, PInst* out) {
+  GfPerm perm(n);
+  std::vector<DTerm> terms;
+  size_t gates = 0;
+  uint64_t support = 0;
+  for (size_t i = i0; i < i1; ++i) {
+    const PInst& in = v[i];
+    if (in.t == IK::Diag) {
+      if (in.dp_n != n) return false;
+      for (uint64_t c : in.conds)
+        if (n < 64 && (c >> n) != 0) return false;
+      for (const aleph_b200_phase_term& t : in.terms) {
+        DTerm d;
+        for (uint32_t c = 0; c < t.cond_count; ++c) {
+          d.conds.push_back(perm.image_of_mask(in.conds[t.cond_offset + c]));
+          support |= d.conds.back();
+        }
+        d.angle = t.angle;
+        terms.push_back(std::move(d));
+      }
+      ++gates;
+      continue;
+    }
+    const PGate& g = in.g;
+    if (g.kind == ALEPH_GATE_CNOT) {
+      if (!g.c.empty() || g.q.size() < 2) return false;
+      perm.cx(g.q[0], g.q[1]);
+      support |= (1ull << g.q[0]) | (1ull << g.q[1]);
+    } else {
+      if (!diagonal_to_terms(g, perm, &terms)) return false;
+      ++gates;
+      for (uint32_t q : g.q) support |= 1ull << q;
+      for (uint32_t c : g.c) support |= 1ull << c;
+    }
+  }
+  if (!perm.identity()) return false;
+  if (__builtin_popcountll(support) <= 1 || gates < 2) return false;
+  // merge terms with the same (sorted) condition set, in key order
+  std::map<std::vector<uint64_t>, double> merged;
+  for (DTerm& t : terms) {
+    std::sort(t.conds.begin(), t.conds.end());
+    auto it = merged.find(t.conds);
+    if (it == merged.end()) merged.emplace(t.conds, t.angle);
+    else it->second += t.angle;
+  }
+  out->t = IK::Diag;
+  out->dp_n = n;
+  out->terms.clear();
+  out->conds.clear();
+  for (const auto& kv : merged) {
+    const double a = rem_2pi(kv.second);
+    if (a < kPhaseEps || 2.0 * M_PI - a < kPhaseEps) continue;
+    aleph_b200_phase_term t;
+    t.angle = kv.second;
+    t.cond_offset = (uint32_t)out->conds.size();
+    t.cond_count = (uint32_t)kv.first.size();
+    out->conds.insert(out->conds.end(), kv.first.begin(), kv.first.end());
+    out->terms.push_back(t);
+  }
+  return true;
+}
+
+// FuseDiagonalRuns::run (fuse_diagonal.rs:23-68): maximal runs of diagonal
+// gates, bare CNOTs and DiagonalPhase records become one DiagonalPhase each.
+void fuse_diagonal_runs(std::vector<PInst>& v, uint32_t n) {
+  std::vector<PInst> out;
+  size_t i = 0;
+  while (i < v.size()) {
+    if (!diag_run_member(v[i])) {
+      out.push_back(std::move(v[i]));
+      ++i;
+      continue;
+    }
+    size_t j = i;
+    while (j < v.size() && diag_run_member(v[j])) ++j;
+    PInst dp;
+    if (fuse_diag_run(v, i, j, n, &dp)) out.push_back(std::move(dp));
+    else
+      for (size_t k = i; k < j; ++k) out.push_back(std::move(v[k]));
+    i = j;
+  }
+  v = std::move(out);
+}
+
 // TileBlock::run (crates/aleph-ir/src/passes/tile_block.rs:47-110)
 void tile_block(std::vector<PInst>& v, uint32_t tile_bits) {
   std::vector<PInst> out;
@@ -1018,6 +1178,32 @@ void plan(std::vector<PInst>& v, uint32_t n, uint32_t tile_bits, uint32_t max_k,
   }
 }
 
+// fuse_full_state (crates/aleph-cuda/src/fusion.rs:137-152), the pass list of
+// the reference's CUDA execution plan (CudaExecutionPlan::compile,
+// crates/aleph-cuda/src/execution.rs:118-126): CancelInversePairs,
+// FuseDiagonalRuns, Fuse1qRuns, Fuse2q, FuseKq (width MAX_FUSE_QUBITS = 3). No
+// relabelling and no tiling. pc->tiled_blocks counts the DiagonalPhase records.
+void plan_gpu(std::vector<PInst>& v, uint32_t n, uint32_t max_k, PassCounts* pc) {
+  pc->input = v.size();
+  pc->relabeled = 0;
+  cancel_inverse_pairs(v);
+  pc->after_cancel = v.size();
+  fuse_diagonal_runs(v, n);
+  fuse_1q_runs(v);
+  pc->after_fuse1q = v.size();
+  fuse_2q(v);
+  pc->after_fuse2q = v.size();
+  fuse_kq(v, n, max_k);
+  pc->after_fusekq = v.size();
+  pc->output = v.size();
+  pc->tiled_blocks = 0;
+  pc->fused_kq = 0;
+  for (const PInst& in : v) {
+    pc->tiled_blocks += in.t == IK::Diag;
+    pc->fused_kq += in.t == IK::Gate && in.g.kind == ALEPH_GATE_UNITARYKQ;
+  }
+}
+
 double now() {
   return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
@@ -1050,7 +1236,102 @@ struct orc_pipeline {
   PassCounts pc{};
   uint32_t n = 0;
   double plan_s = 0;
+  // the planned list as flat records (orc_pipeline_records)
+  std::vector<aleph_b200_instr> rec;
+  std::vector<double> mpool;
+  std::vector<aleph_b200_phase_term> tpool;
+  std::vector<uint64_t> cpool;
 };
+
+/* The reference's CUDA pass list (fuse_full_state) on a record stream; the
+ * result runs on the CPU through orc_pipeline_exec or is exported as records
+ * for the GPU reference arm (ref_gpu.cpp). */
+int orc_gpu_pipeline_plan(uint32_t n, const aleph_b200_instr* instrs, uint64_t count, const aleph_b200_pools* pools,
+                          uint32_t max_k, orc_pipeline** out) {
+  const double t0 = now();
+  auto* P = new orc_pipeline();
+  P->n = n;
+  if (int s = parse(instrs, count, pools, &P->v)) {
+    delete P;
+    return s;
+  }
+  plan_gpu(P->v, n, max_k, &P->pc);
+  P->plan_s = now() - t0;
+  *out = P;
+  return ALEPH_B200_OK;
+}
+
+/* The planned instructions as flat records and pools (owned by the plan).
+ * Gates carry their matrix (Unitary*, UnitaryKq) in the matrix pool. */
+int orc_pipeline_records(orc_pipeline* P, const aleph_b200_instr** instrs, uint64_t* count, aleph_b200_pools* pools) {
+  P->rec.clear();
+  P->mpool.clear();
+  P->tpool.clear();
+  P->cpool.clear();
+  for (const PInst& in : P->v) {
+    aleph_b200_instr r{};
+    switch (in.t) {
+      case IK::Gate: {
+        const PGate& g = in.g;
+        r.kind = g.kind;
+        r.num_qubits = (uint32_t)std::min<size_t>(g.q.size(), 8);
+        r.num_controls = (uint32_t)std::min<size_t>(g.c.size(), 8);
+        for (uint32_t i = 0; i < r.num_qubits; ++i) r.qubits[i] = g.q[i];
+        for (uint32_t i = 0; i < r.num_controls; ++i) r.controls[i] = g.c[i];
+        std::memcpy(r.params, g.p, sizeof(r.params));
+        r.aux = g.k;
+        r.data_offset = P->mpool.size() / 2;
+        r.data_len = g.data.size();
+        for (const C& z : g.data) {
+          P->mpool.push_back(z.real());
+          P->mpool.push_back(z.imag());
+        }
+        break;
+      }
+      case IK::Diag:
+        r.kind = ALEPH_INSTR_DIAGONAL_PHASE;
+        r.aux = in.dp_n;
+        r.data_offset = P->tpool.size();
+        r.data_len = in.terms.size();
+        for (aleph_b200_phase_term t : in.terms) {
+          t.cond_offset += (uint32_t)P->cpool.size();
+          P->tpool.push_back(t);
+        }
+        P->cpool.insert(P->cpool.end(), in.conds.begin(), in.conds.end());
+        break;
+      case IK::Measure:
+        r.kind = ALEPH_INSTR_MEASURE;
+        r.num_qubits = 1;
+        r.qubits[0] = in.qubit;
+        r.aux = in.clbit;
+        break;
+      case IK::Barrier:
+        r.kind = ALEPH_INSTR_BARRIER;
+        for (uint32_t q : in.qs) r.data_offset |= 1ull << q;
+        break;
+      default:
+        return ALEPH_B200_UNSUPPORTED_INSTRUCTION;
+    }
+    P->rec.push_back(r);
+  }
+  *instrs = P->rec.data();
+  *count = P->rec.size();
+  pools->matrix_pool = P->mpool.data();
+  pools->matrix_pool_len = P->mpool.size() / 2;
+  pools->terms = P->tpool.data();
+  pools->n_terms = P->tpool.size();
+  pools->cond_pool = P->cpool.data();
+  pools->n_conds = P->cpool.size();
+  return ALEPH_B200_OK;
+}
+
+/* Pass counts of a plan (the layout of orc_pipeline_describe's output). */
+void orc_pipeline_counts(const orc_pipeline* P, uint64_t* out) {
+  const PassCounts& pc = P->pc;
+  const uint64_t o[9] = {pc.input, pc.after_cancel, pc.after_fuse1q, pc.after_fuse2q, pc.after_fusekq,
+                         pc.output, pc.tiled_blocks, pc.fused_kq, pc.relabeled};
+  std::memcpy(out, o, sizeof(o));
+}
 
 int orc_pipeline_plan(uint32_t n, const aleph_b200_instr* instrs, uint64_t count, const aleph_b200_pools* pools,
                       uint32_t tile_bits, uint32_t max_k, orc_pipeline** out) {

@@ -186,3 +186,62 @@ def test_sliced_execution_equals_whole():
     P.free()
     assert np.abs(psi - whole).max() == 0.0
     assert math.isclose(float(np.vdot(psi, psi).real), 1.0, abs_tol=1e-12)
+
+
+# ---- the reference's CUDA pass list (fuse_full_state), executed on the CPU kernels ----------
+def gpu_plan_state(n, insts):
+    plan = oracle.PlannedCircuit(n, insts, max_k=3, gpu=True)
+    psi = oracle.zero_state(n)
+    plan.execute(psi)
+    return psi, plan.counts()
+
+
+@pytest.mark.parametrize("make", [
+    lambda: (10, workloads.brickwall(10, 8, seed=4).instructions),
+    lambda: (9, workloads.qft_product(9, seed=2).instructions),
+    lambda: (8, workloads.grover(3, 5, 2).instructions),
+    lambda: (9, random_circuit(9, 160, seed=11).instructions),
+    lambda: (7, random_circuit(7, 300, seed=12).instructions),
+])
+def test_gpu_pass_list_matches_the_raw_oracle(make):
+    n, insts = make()
+    want, _ = oracle.run(n, insts)
+    got, _ = gpu_plan_state(n, insts)
+    assert np.abs(got - want).max() <= TOL
+
+
+def test_fuse_diagonal_runs_one_phase_per_cz_layer():
+    # every CZ layer of the brickwall is a run of diagonal gates between two
+    # Haar layers: one DiagonalPhase each (fuse_diagonal.rs:23-68)
+    n, depth = 12, 10
+    _, k = gpu_plan_state(n, workloads.brickwall(n, depth, seed=1).instructions)
+    assert k["tiled_blocks"] == depth
+    assert k["fused_kq"] == 0  # disjoint one-qubit gates never share a FuseKq block
+
+
+def test_fuse_diagonal_runs_absorbs_cnot_conjugation():
+    # CNOT(0,1) Rz(0.3) on 1 CNOT(0,1): net permutation identity, two diagonal
+    # members -> one DiagonalPhase over parity(b0 ^ b1); a lone Rz is left alone
+    c = C.Circuit(3).add(C.Cnot(), [0, 1]).add(C.Rz(0.3), [1]).add(C.Cnot(), [0, 1]).add(C.Cz(), [1, 2])
+    got, k = gpu_plan_state(3, c.instructions)
+    assert k["tiled_blocks"] == 1 and k["output"] == 1
+    want, _ = oracle.run(3, c.instructions)
+    assert np.abs(got - want).max() <= TOL
+    lone = C.Circuit(2).add(C.Rz(0.3), [1])
+    assert gpu_plan_state(2, lone.instructions)[1]["tiled_blocks"] == 0
+    # a run whose CNOTs do not cancel is emitted as it is
+    odd = C.Circuit(2).add(C.Cnot(), [0, 1]).add(C.Rz(0.3), [1]).add(C.Cz(), [0, 1])
+    got, k = gpu_plan_state(2, odd.instructions)
+    assert k["tiled_blocks"] == 0
+    assert np.abs(got - oracle.run(2, odd.instructions)[0]).max() <= TOL
+
+
+def test_gpu_pass_list_on_the_golden_fixtures():
+    for fx in load_reference_fixtures():
+        name = fx["name"]
+        insts = fixture_instructions(fx)
+        if any(isinstance(i, C.Measure) for i in insts):
+            continue
+        n = fx["num_qubits"]
+        got, _ = gpu_plan_state(n, insts)
+        assert np.abs(got - fixture_state(fx)).max() <= 1e-10, name
