@@ -745,6 +745,22 @@ def run_engine(args, ranks: Ranks):
         s64_per = ms64 * 1e-3 / (args.fp64_steps * ranks.world)
         fp64 = {"s_per_circuit": s64_per, "steps": args.fp64_steps, "tc32_speedup": s64_per / s_per_circuit,
                 "kernels": kernel_table(per64, peak)}
+        # The plain FP64 passes fuse many gates each, so their roofline is
+        # max(bytes / HBM, DFMA / the FP64 rate), with the DFMA rate measured
+        # on this GPU (aleph_b200_fp64_rate). Every Haar one-qubit gate costs
+        # 8 DFMA per amplitude (two complex products per output); the CZs are
+        # sign flips.
+        rate = b64.fp64_rate()  # TFLOP/s, 2 flop per DFMA
+        n1q = n * depth
+        dfma = 8.0 * n1q * float(1 << n)
+        dfma_s = dfma * 2.0 / (rate * 1e12)
+        passes64 = sum(k["launches"] for k in fp64["kernels"].values()) / max(1, args.fp64_steps)
+        hbm_s = passes64 * 2.0 * float(1 << n) * 16.0 / (peak * 1e9)
+        fp64["roofline"] = {"bound": "max(hbm, fp64)", "fp64_tflops_measured": round(rate, 2), "dfma": dfma,
+                            "dfma_floor_s": round(dfma_s, 4), "hbm_floor_s": round(hbm_s, 4),
+                            "passes": passes64, "frac": round(max(dfma_s, hbm_s) / s64_per, 4),
+                            "what": f"{n1q} Haar gates x 8 DFMA x 2^{n} amplitudes at the measured DFMA rate; "
+                                    f"passes x 2 x 2^{n} x 16 B at the measured HBM copy rate"}
         p64.free()
         s64.free()
         b64.close()
