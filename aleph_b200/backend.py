@@ -277,6 +277,13 @@ class B200SvBackend:
         self._check(self.lib.aleph_b200_norm_sqr(self.handle, state.ptr, ct.byref(out)))
         return out.value
 
+    def state_memory(self, state: State) -> tuple[int, int]:
+        """(device pointer, bytes) of the state's amplitudes, ordered on the
+        handle's stream (``stream_ptr``)."""
+        ptr, nbytes = ct.c_void_p(), ct.c_uint64()
+        self._check(self.lib.aleph_b200_state_memory(self.handle, state.ptr, ct.byref(ptr), ct.byref(nbytes)))
+        return int(ptr.value or 0), int(nbytes.value)
+
     def reset_state(self, state: State) -> None:
         """Back to |0...0> on the device, reusing the allocation."""
         self._check(self.lib.aleph_b200_reset_state(self.handle, state.ptr))

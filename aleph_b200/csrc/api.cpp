@@ -1834,6 +1834,20 @@ int aleph_b200_set_amplitudes(aleph_b200_handle* h, aleph_b200_state* st, const 
   return ALEPH_B200_OK;
 }
 
+int aleph_b200_state_memory(aleph_b200_handle* h, aleph_b200_state* st, void** device_ptr, uint64_t* bytes) {
+  if (!h || !st || !device_ptr || !bytes) return ALEPH_B200_INVALID_ARGUMENT;
+  *device_ptr = st->amps;
+  *bytes = st->bytes;
+  return ALEPH_B200_OK;
+}
+
+int aleph_b200_gate_matrix(const aleph_b200_instr* g, const double* matrix_pool, uint64_t pool_len, double* out,
+                           int* dim) {
+  if (!g || !out || !dim) return ALEPH_B200_INVALID_ARGUMENT;
+  aleph_b200_error_info e{};
+  return gate_matrix_dense(*g, matrix_pool, pool_len, out, dim, &e);
+}
+
 int aleph_b200_norm_sqr(aleph_b200_handle* h, aleph_b200_state* st, double* out) {
   if (!h || !st || !out) return ALEPH_B200_INVALID_ARGUMENT;
   if (int r = bind(h)) return r;

@@ -304,6 +304,10 @@ constexpr uint32_t kBlockImageBytes = 65536;
 // tiled: the gate is one of a TiledBlock's gates, validated as the
 // reference's tiled executor does (fixed-size 2x2 / 4x4 matrix, no
 // unitarity check)
+// Gate::matrix as a dense row-major complex matrix (interleaved re, im),
+// dim 2, 4 or 8 in *dim; UnitaryKq is rejected (it has no fixed-size matrix).
+int gate_matrix_dense(const aleph_b200_instr& g, const double* pool, uint64_t pool_len, double* out, int* dim,
+                      aleph_b200_error_info* e);
 int lower_gate(const aleph_b200_instr& g, uint32_t n, const double* pool, uint64_t pool_len, Lowered* out,
                aleph_b200_error_info* err, bool tiled = false);
 int lower_diagonal_phase(const aleph_b200_phase_term* terms, uint64_t n_terms, const uint64_t* conds, uint64_t n_conds,

@@ -302,6 +302,20 @@ void lower_matrix(const Cx* m, int dim, const uint32_t* tq, uint64_t ctrl, Lower
 
 }  // namespace
 
+int gate_matrix_dense(const aleph_b200_instr& g, const double* pool, uint64_t pool_len, double* out, int* dim,
+                      aleph_b200_error_info* e) {
+  Cx m[8][8];
+  const int d = matrix_of(g, pool, pool_len, m, e);
+  if (d == 0) return e->status ? e->status : ALEPH_B200_UNSUPPORTED_GATE;
+  for (int i = 0; i < d; ++i)
+    for (int j = 0; j < d; ++j) {
+      out[2 * (i * d + j)] = m[i][j].re;
+      out[2 * (i * d + j) + 1] = m[i][j].im;
+    }
+  *dim = d;
+  return ALEPH_B200_OK;
+}
+
 const char* gate_name(uint32_t kind) {
   static const char* names[] = {"H",   "X",   "Y",   "Z",   "S",     "Sdg",     "T",       "Tdg",
                                 "Rx",  "Ry",  "Rz",  "Phase", "U3",  "Cnot",    "Cz",      "Swap",

@@ -219,14 +219,19 @@ class LearnedPlanner:
 
 # ---- measurement, data collection and the autotuner -----------------------------------
 def state_signature(backend: B200SvBackend, st, n: int) -> np.ndarray:
-    """What the autotuner compares between plans: the amplitudes up to n = 26,
-    else the marginal distributions of the lowest and the highest 10 qubits."""
+    """What the autotuner compares between plans: the amplitudes up to n = 26;
+    above that, eight windows of 4096 amplitudes spread over the state (at
+    fixed seeded offsets) plus the marginal distributions of the lowest and
+    the highest 10 qubits."""
     if n <= 26:
         return backend.statevector(st)
+    rng = np.random.default_rng(n)
+    starts = [0, (1 << n) - 4096] + [int(x) * 4096 for x in rng.integers(0, (1 << n) // 4096, 6)]
+    amps = np.concatenate([backend.amplitude_range(st, a, 4096) for a in starts])
     k = min(10, n)
     lo = backend.probabilities(st, list(range(k)))
     hi = backend.probabilities(st, list(range(n - k, n)))
-    return np.concatenate([lo, hi])
+    return np.concatenate([amps, lo, hi])
 
 
 def measure(backend: B200SvBackend, n: int, flat: Flat, choice: PlanChoice, repeats: int = 2):
@@ -312,15 +317,16 @@ MODEL_PATH = Path(__file__).resolve().parent / "cost_model.npz"
 
 
 # ---- training set and held-out evaluation ------------------------------------------------
-def training_circuits(scale: int = 0, seed: int = 0):
-    """Generated training circuits: random brickwall, QFT, QAOA p = 1..6 on
-    random 3-regular graphs and Grover (multi-controlled Z in CX + T), at
-    n = 20 + scale .. 26 + scale qubits."""
+def training_circuits(sizes=(22, 26, 30), seed: int = 0):
+    """Generated training circuits at each size n: random brickwall (depth
+    10, 25, 60), the textbook QFT on a product state, QAOA p = 1, 3, 6 on
+    random 3-regular graphs, and Grover (multi-controlled Z in CX + T) with
+    n/2 + 1 data qubits and 2 iterations."""
     from . import workloads as W
 
     rng = np.random.default_rng(seed)
     out = []
-    for n in (20 + scale, 23 + scale, 26 + scale):
+    for n in sizes:
         for d in (10, 25, 60):
             out.append((n, W.brickwall(n, d, seed=int(rng.integers(1 << 30))).instructions))
         out.append((n, W.qft_product(n, seed=int(rng.integers(1 << 30))).instructions))
@@ -328,38 +334,72 @@ def training_circuits(scale: int = 0, seed: int = 0):
         for p in (1, 3, 6):
             edges = W.random_3_regular(m, rng)
             out.append((m, W.qaoa_maxcut(m, edges, rng.uniform(0, np.pi, p), rng.uniform(0, np.pi, p)).instructions))
-    for nd in (10 + scale // 2, 12 + scale // 2):
+        nd = n // 2 + 1
         out.append((2 * nd - 2, W.grover(nd, int(rng.integers(1 << nd)), 2).instructions))
     return out
 
 
-def heldout_circuits(n_brick: int = 28, n_grover_data: int = 14, seed: int = 1):
-    """Held-out evaluation: a depth-40 random brickwall, Grover (20
-    iterations) and the textbook QFT on a product state (none of them in the
-    training set with these sizes and seeds)."""
+def large_training_circuits(precision: str, seed: int = 7):
+    """Pass samples at the top of the engine's range (FP64 to n = 33, FP32 and
+    TC32 to n = 32): the depth-10 brickwall and the QFT. These states are 64
+    to 128 GiB, so they run under the few candidates of ``large_choices``."""
     from . import workloads as W
 
     rng = np.random.default_rng(seed)
-    return [("brickwall", n_brick, W.brickwall(n_brick, 40, seed=seed).instructions),
-            ("grover", 2 * n_grover_data - 2, W.grover(n_grover_data, int(rng.integers(1 << n_grover_data)), 20).instructions),
-            ("qft", n_brick, W.qft_product(n_brick, seed=seed).instructions)]
+    sizes = (32, 33) if precision == "f64" else (31, 32)
+    out = []
+    for n in sizes:
+        out.append((n, W.brickwall(n, 10, seed=int(rng.integers(1 << 30))).instructions))
+        out.append((n, W.qft_product(n, seed=int(rng.integers(1 << 30))).instructions))
+    return out
 
 
-def evaluate(model_path, heldout_n: int = 28, heldout_grover: int = 14) -> list:
+def large_choices(precision: str) -> list[PlanChoice]:
+    """The candidates sampled at the largest sizes: the greedy configuration
+    and its nearest neighbours (4 and 3 register qubits, the other occupancy
+    variants at 4)."""
+    c = candidates(precision)
+    if precision == "tc32":
+        return c[:2] + [x for x in c[2:] if x.tile_r == 5][:2]
+    default = default_occupancy(precision)
+    # FP64 tiles at 5 register qubits spill above two blocks per SM: left out here
+    return [x for x in c if x.tile_r == 4 or (x.tile_r == 5 and (precision != "f64" or x.tile_occupancy in (0, default)))]
+
+
+def heldout_circuits(precision: str, n_brick: int | None = None, n_grover_data: int = 16, n_qft: int = 30,
+                     seed: int = 1):
+    """Held-out evaluation circuits at the configured sizes (none of them in
+    the training set): a depth-40 random brickwall (n = 33 for FP64, 32 for
+    FP32 / TC32), Grover with 16 data qubits (30 qubits with the ancillas) and
+    20 iterations, and the textbook QFT on a product state at n = 30."""
+    from . import workloads as W
+
+    rng = np.random.default_rng(seed)
+    nb = n_brick or (33 if precision == "f64" else 32)
+    return [("brickwall", nb, W.brickwall(nb, 40, seed=seed).instructions),
+            ("grover", 2 * n_grover_data - 2,
+             W.grover(n_grover_data, int(rng.integers(1 << n_grover_data)), 20).instructions),
+            ("qft", n_qft, W.qft_product(n_qft, seed=seed).instructions)]
+
+
+def evaluate(model_path, precisions=("f64", "tc32"), **heldout_kw) -> list:
     """The learned planner (autotuned: kept only if measured faster and
     state-equal) against the greedy plan on the held-out circuits."""
     evals = []
-    for prec in ("f64", "tc32"):
+    for prec in precisions:
         bq = B200SvBackend(seed=0, precision=prec)
         mq = CostModel.load(bq, model_path)
         planner = LearnedPlanner(mq)
-        for name, n, instr in heldout_circuits(heldout_n, heldout_grover):
-            scored = planner.score(n, instr, prec)
-            res = autotune(bq, n, instr, planner, top_k=2)
-            evals.append({"precision": prec, "circuit": name, "n": n,
+        for name, n, instr in heldout_circuits(prec, **heldout_kw):
+            flat = flatten(instr)
+            scored = planner.score(n, flat, prec)
+            res = autotune(bq, n, flat, planner, top_k=2)
+            evals.append({"precision": prec, "circuit": name, "n": n, "gates": int(flat.n),
                           "greedy_ms": round(res.greedy_ms, 3), "learned_ms": round(res.chosen_ms, 3),
                           "gain": round(res.greedy_ms / res.chosen_ms, 4), "choice": res.choice.__dict__,
                           "top_predicted": [(s.choice.__dict__, round(s.predicted_ms, 2)) for s in scored[:3]],
+                          "greedy_predicted_ms": round(next(s.predicted_ms for s in scored if s.choice == GREEDY), 2),
+                          "measured": {str(k.__dict__): round(v, 3) for k, v in res.measured.items()},
                           "rejected": [str(r[1]) for r in res.rejected]})
         mq.free()
         bq.close()
@@ -368,10 +408,12 @@ def evaluate(model_path, heldout_n: int = 28, heldout_grover: int = 14) -> list:
 
 def main(argv=None) -> int:
     """python -m aleph_b200.learned [--out PATH] [--epochs E]: collect pass
-    timings on the GPU (f64, f32 and tc32 handles), train the cost model,
-    evaluate the learned planner against the greedy plan on held-out circuits,
-    print one JSON summary and save the model. With --eval-only: the held-out
-    evaluation of the model at --out, without collecting or training."""
+    timings on the GPU (f64, f32 and tc32 handles; n = 22..30 under every
+    candidate configuration, n = 31..33 under the few of ``large_choices``),
+    train the cost model, evaluate the learned planner against the greedy
+    plan on the held-out circuits, print one JSON summary and save the model.
+    With --eval-only: the held-out evaluation of the model at --out, without
+    collecting or training."""
     import argparse
     import json
     import time
@@ -379,22 +421,32 @@ def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=str(MODEL_PATH))
     ap.add_argument("--epochs", type=int, default=300)
-    ap.add_argument("--scale", type=int, default=0)
-    ap.add_argument("--heldout-n", type=int, default=28)
-    ap.add_argument("--heldout-grover", type=int, default=14)
+    ap.add_argument("--sizes", default="22,26,30")
+    ap.add_argument("--no-large", action="store_true", help="skip the n = 31..33 samples")
+    ap.add_argument("--heldout-brick", type=int, default=0, help="brickwall qubits (0: 33 FP64 / 32 TC32)")
+    ap.add_argument("--heldout-grover", type=int, default=16)
+    ap.add_argument("--heldout-qft", type=int, default=30)
     ap.add_argument("--eval-only", action="store_true")
     args = ap.parse_args(argv)
+    hk = {"n_brick": args.heldout_brick or None, "n_grover_data": args.heldout_grover, "n_qft": args.heldout_qft}
     if args.eval_only:
-        print(json.dumps({"model": str(args.out), "heldout": evaluate(args.out, args.heldout_n, args.heldout_grover)}))
+        print(json.dumps({"model": str(args.out), "heldout": evaluate(args.out, **hk)}))
         return 0
     t0 = time.perf_counter()
     Xs, ys = [], []
-    circuits = training_circuits(args.scale)
+    circuits = training_circuits(tuple(int(x) for x in args.sizes.split(",")))
+    n_large = 0
     for prec in ("f64", "f32", "tc32"):
         be = B200SvBackend(seed=0, precision=prec)
         X, y = collect(be, circuits)
         Xs.append(X)
         ys.append(y)
+        if not args.no_large:
+            big = large_training_circuits(prec)
+            X, y = collect(be, big, large_choices(prec))
+            Xs.append(X)
+            ys.append(y)
+            n_large += len(y)
         be.close()
     X, y = np.concatenate(Xs), np.concatenate(ys)
     t_collect = time.perf_counter() - t0
@@ -409,11 +461,13 @@ def main(argv=None) -> int:
     val_rmse = float(np.sqrt(np.mean((pred - y[val]) ** 2)))
     base_rmse = float(np.sqrt(np.mean((y[val] - y[~val].mean()) ** 2)))
     model.save(args.out)
-    evals = evaluate(args.out, args.heldout_n, args.heldout_grover)
-    print(json.dumps({"samples": int(len(y)), "circuits": len(circuits), "collect_s": round(t_collect, 1),
-                      "train_s": round(t_train, 2), "train_samples_per_s": round(args.epochs * (~val).sum() / t_train),
+    t2 = time.perf_counter()
+    evals = evaluate(args.out, **hk)
+    print(json.dumps({"samples": int(len(y)), "large_samples": int(n_large), "circuits": len(circuits),
+                      "collect_s": round(t_collect, 1), "train_s": round(t_train, 2),
+                      "train_samples_per_s": round(args.epochs * (~val).sum() / t_train),
                       "final_batch_loss": loss, "val_rmse_log": val_rmse, "val_rmse_mean_predictor": base_rmse,
-                      "heldout": evals}))
+                      "eval_s": round(time.perf_counter() - t2, 1), "heldout": evals}))
     model.free()
     be.close()
     return 0

@@ -321,6 +321,21 @@ int aleph_b200_get_amplitudes(aleph_b200_handle* h, aleph_b200_state* st, double
 int aleph_b200_get_amplitude_range(aleph_b200_handle* h, aleph_b200_state* st, uint64_t first, uint64_t count,
                                    double* out);
 int aleph_b200_set_amplitudes(aleph_b200_handle* h, aleph_b200_state* st, const double* in);
+/* The state's device memory (2^n interleaved complex128, or complex64 for
+ * F32/TC32 handles) and its size in bytes, ordered on the handle's stream
+ * (aleph_b200_get_stream). For callers that move amplitudes between states or
+ * GPUs themselves: the distributed layer's global-qubit exchanges send and
+ * receive halves of it over NCCL (DeviceSv::amps_view / amps_view_mut,
+ * crates/aleph-cuda/src/dist/mod.rs:49-62). */
+int aleph_b200_state_memory(aleph_b200_handle* h, aleph_b200_state* st, void** device_ptr, uint64_t* bytes);
+
+/* ---- Gate::matrix (crates/aleph-core/src/gate/kinds.rs:213-400) ----
+ * The dense matrix of one gate record (dim 2, 4 or 8, row-major, interleaved
+ * re/im, MSB-first operand order) into out[2 * dim * dim]; UnitaryKq records
+ * are rejected like the reference's Gate::matrix (no fixed-size matrix). */
+int aleph_b200_gate_matrix(const aleph_b200_instr* g, const double* matrix_pool, uint64_t pool_len, double* out,
+                           int* dim);
+
 /* FP64 sum of |a_i|^2 on the device. */
 int aleph_b200_norm_sqr(aleph_b200_handle* h, aleph_b200_state* st, double* out);
 
