@@ -216,6 +216,7 @@ _SIGNATURES = {
     "aleph_b200_get_amplitude_range": ([_P, _P, ct.c_uint64, ct.c_uint64, ct.POINTER(ct.c_double)], ct.c_int),
     "aleph_b200_fp64_rate": ([_P, ct.POINTER(ct.c_double)], ct.c_int),
     "aleph_b200_state_memory": ([_P, _P, ct.POINTER(ct.c_void_p), ct.POINTER(ct.c_uint64)], ct.c_int),
+    "aleph_b200_scale_state": ([_P, _P, ct.c_double], ct.c_int),
     "aleph_b200_gate_matrix": ([ct.POINTER(Instr), ct.POINTER(ct.c_double), ct.c_uint64, ct.POINTER(ct.c_double),
                                 ct.POINTER(ct.c_int)], ct.c_int),
     "aleph_b200_set_amplitudes": ([_P, _P, ct.POINTER(ct.c_double)], ct.c_int),

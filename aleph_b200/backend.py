@@ -284,6 +284,10 @@ class B200SvBackend:
         self._check(self.lib.aleph_b200_state_memory(self.handle, state.ptr, ct.byref(ptr), ct.byref(nbytes)))
         return int(ptr.value or 0), int(nbytes.value)
 
+    def scale_state(self, state: State, factor: float) -> None:
+        """Every amplitude times ``factor`` (> 0), on the device."""
+        self._check(self.lib.aleph_b200_scale_state(self.handle, state.ptr, float(factor)))
+
     def reset_state(self, state: State) -> None:
         """Back to |0...0> on the device, reusing the allocation."""
         self._check(self.lib.aleph_b200_reset_state(self.handle, state.ptr))

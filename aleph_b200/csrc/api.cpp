@@ -1841,6 +1841,18 @@ int aleph_b200_state_memory(aleph_b200_handle* h, aleph_b200_state* st, void** d
   return ALEPH_B200_OK;
 }
 
+int aleph_b200_scale_state(aleph_b200_handle* h, aleph_b200_state* st, double factor) {
+  if (!h || !st || !(factor > 0.0) || !std::isfinite(factor)) return ALEPH_B200_INVALID_ARGUMENT;
+  if (int r = bind(h)) return r;
+  if (int r = ensure(h, h->reduce, 256)) return r;
+  const double norm2 = 1.0 / (factor * factor);  // the rescale kernel multiplies by 1 / sqrt(norm2)
+  CK(copy_async(h, h->reduce.ptr, &norm2, sizeof(norm2), cudaMemcpyHostToDevice, h->stream), "scale upload");
+  CK(launch_rescale(st->amps, st->precision, st->n, (const double*)h->reduce.ptr, h->stream), "rescale");
+  CK(cudaStreamSynchronize(h->stream), "stream synchronize");
+  h->stats.kernel_launches += 1;
+  return ALEPH_B200_OK;
+}
+
 int aleph_b200_gate_matrix(const aleph_b200_instr* g, const double* matrix_pool, uint64_t pool_len, double* out,
                            int* dim) {
   if (!g || !out || !dim) return ALEPH_B200_INVALID_ARGUMENT;
@@ -1904,6 +1916,10 @@ int aleph_b200_set_tuning(aleph_b200_handle* h, const char* key, int64_t value) 
     if (value != 0 && (value < 2 || value > 4))
       return set_error(h, ALEPH_B200_INVALID_ARGUMENT, "tile_occupancy must be 0 or in 2..4");
     h->opts.tile_occupancy = (uint32_t)value;
+    return ALEPH_B200_OK;
+  }
+  if (!std::strcmp(key, "renormalize")) {
+    h->opts.renormalize = value != 0;
     return ALEPH_B200_OK;
   }
   if (!std::strcmp(key, "tensor_blocks")) {

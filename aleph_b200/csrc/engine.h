@@ -149,6 +149,7 @@ struct PlanOptions {
   bool block_window_search = true;  // TC32: also try every 6-qubit window per pass
   uint32_t tile_occupancy = 0;      // tile kernel variant: 128-thread blocks per SM (0 = 2)
   bool relabel_swaps = true;        // SWAPs relabel qubits; one permutation pass settles the map
+  bool renormalize = true;          // TC32: rescale to norm 1 after a stream's block passes
 };
 
 // ---------------------------------------------------------------------------
@@ -224,6 +225,8 @@ cudaError_t launch_kq_pass(void* amps, int precision, uint32_t n, const Op* op_d
                            const void* coef, cudaStream_t s);
 cudaError_t launch_block_pass(void* amps, const BlockPass& p, const uint8_t* images, const Op* ops,
                               const void* coef, PolyTables poly, int* dev_error, int sm_count, cudaStream_t s);
+// amps *= 1 / sqrt(*norm2) (norm2 in device memory).
+cudaError_t launch_rescale(void* amps, int precision, uint32_t n, const double* norm2, cudaStream_t s);
 cudaError_t launch_renormalize(void* amps, int precision, uint32_t n, double* partials, uint32_t nblocks, double* out2,
                                cudaStream_t s);
 cudaError_t launch_convert(const void* src, int src_prec, void* dst, int dst_prec, uint64_t count, cudaStream_t s);

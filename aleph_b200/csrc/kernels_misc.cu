@@ -428,6 +428,15 @@ __global__ void rescale_kernel(V2<Real>* __restrict__ amps, uint64_t len, const 
   }
 }
 
+cudaError_t launch_rescale(void* amps, int precision, uint32_t n, const double* norm2, cudaStream_t s) {
+  const uint64_t len = 1ull << n;
+  const uint64_t b = (len + 255) / 256;
+  const unsigned blocks = (unsigned)(b > 148ull * 32 ? 148ull * 32 : b);
+  if (precision == ALEPH_B200_F64) rescale_kernel<double><<<blocks, 256, 0, s>>>((double2*)amps, len, norm2);
+  else rescale_kernel<float><<<blocks, 256, 0, s>>>((float2*)amps, len, norm2);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_renormalize(void* amps, int precision, uint32_t n, double* partials, uint32_t nblocks, double* out2,
                                cudaStream_t s) {
   cudaError_t e = launch_norm(amps, precision, n, partials, nblocks, out2, s);

@@ -62,6 +62,55 @@ __device__ __forceinline__ void reg_1q(V2<Real> (&v)[1 << R], const V2<Real>* m,
   }
 }
 
+// Two one-qubit gates in a row, U1 on register bit J1 then U2 on register bit
+// J2 != J1, neither controlled: one sweep over quartets. U1 writes four
+// temporaries and U2 writes straight back into the loop-carried registers,
+// so no amplitude moves between the two gates (a lone gate must park three
+// of every four results while its inputs are still live).
+template <typename Real, int R, int J1, int J2>
+__device__ __forceinline__ void reg_1q_pair(V2<Real> (&v)[1 << R], const V2<Real>* m, const V2<Real>* u) {
+  const V2<Real> m0 = ld_coef<Real>(m), m1 = ld_coef<Real>(m + 1), m2 = ld_coef<Real>(m + 2),
+                 m3 = ld_coef<Real>(m + 3);
+  const V2<Real> u0 = ld_coef<Real>(u), u1 = ld_coef<Real>(u + 1), u2 = ld_coef<Real>(u + 2),
+                 u3 = ld_coef<Real>(u + 3);
+  constexpr int B1 = 1 << J1, B2 = 1 << J2;
+#pragma unroll
+  for (int r = 0; r < (1 << R); ++r) {
+    if (r & (B1 | B2)) continue;
+    const V2<Real> x00 = v[r], x01 = v[r | B1], x10 = v[r | B2], x11 = v[r | B1 | B2];
+    const V2<Real> t00 = cmul2<Real>(m0, x00, m1, x01), t01 = cmul2<Real>(m2, x00, m3, x01);
+    const V2<Real> t10 = cmul2<Real>(m0, x10, m1, x11), t11 = cmul2<Real>(m2, x10, m3, x11);
+    v[r] = cmul2<Real>(u0, t00, u1, t10);
+    v[r | B2] = cmul2<Real>(u2, t00, u3, t10);
+    v[r | B1] = cmul2<Real>(u0, t01, u1, t11);
+    v[r | B1 | B2] = cmul2<Real>(u2, t01, u3, t11);
+  }
+}
+
+// Sign flip of the registers r with (r & K) == K: a CZ-like op whose
+// register part K is known at compile time runs without per-amplitude tests.
+template <typename Real, int R, uint32_t K>
+__device__ __forceinline__ void reg_neg(V2<Real> (&v)[1 << R]) {
+#pragma unroll
+  for (int r = 0; r < (1 << R); ++r)
+    if (((uint32_t)r & K) == K) v[r] = cneg<Real>(v[r]);
+}
+
+template <typename Real, int R>
+__device__ __forceinline__ void dispatch_neg(V2<Real> (&v)[1 << R], uint32_t creg) {
+#define AB_NEG(k) \
+  case k:         \
+    if constexpr ((k) < (1u << R)) reg_neg<Real, R, k>(v); \
+    break;
+  switch (creg) {
+    AB_NEG(0) AB_NEG(1) AB_NEG(2) AB_NEG(3) AB_NEG(4) AB_NEG(5) AB_NEG(6) AB_NEG(7)
+    AB_NEG(8) AB_NEG(9) AB_NEG(10) AB_NEG(11) AB_NEG(12) AB_NEG(13) AB_NEG(14) AB_NEG(15)
+    AB_NEG(16) AB_NEG(17) AB_NEG(18) AB_NEG(19) AB_NEG(20) AB_NEG(21) AB_NEG(22) AB_NEG(23)
+    AB_NEG(24) AB_NEG(25) AB_NEG(26) AB_NEG(27) AB_NEG(28) AB_NEG(29) AB_NEG(30) AB_NEG(31)
+  }
+#undef AB_NEG
+}
+
 template <typename Real, int R, int J>
 __device__ __forceinline__ void reg_x(V2<Real> (&v)[1 << R], bool thr, uint32_t creg) {
 #pragma unroll
@@ -174,13 +223,9 @@ __device__ __forceinline__ void diag_ops(const Op& op, V2<Real> (&v)[1 << R], ui
                                          const V2<Real>* coef, const PolyTables& poly) {
   const uint32_t creg = op.creg;
   switch (op.type) {
-    case OP_NEG: {
-      const bool thr = (gl & op.mask) == op.mask;
-#pragma unroll
-      for (int r = 0; r < (1 << R); ++r)
-        if (AB_ON(r)) v[r] = cneg<Real>(v[r]);
+    case OP_NEG:
+      if ((gl & op.mask) == op.mask) dispatch_neg<Real, R>(v, creg);
       break;
-    }
     case OP_CPHASE: {
       const bool thr = (gl & op.mask) == op.mask;
       const V2<Real> c = ld_coef<Real>(coef + op.coef);
@@ -239,6 +284,22 @@ __device__ __forceinline__ void dispatch_reg(const Op& op, V2<Real> (&v)[1 << R]
     case 3: if constexpr (R > 3) reg_1q<Real, R, 3>(v, m, thr, creg); break;
     case 4: if constexpr (R > 4) reg_1q<Real, R, 4>(v, m, thr, creg); break;
   }
+}
+
+// Two uncontrolled one-qubit gates on register bits j1 != j2 (in that order).
+template <typename Real, int R>
+__device__ __forceinline__ void dispatch_pair(int j1, int j2, V2<Real> (&v)[1 << R], const V2<Real>* m,
+                                              const V2<Real>* u) {
+#define AB_PR(a, b)                                                      \
+  case (a)*8 + (b):                                                      \
+    if constexpr (R > (a) && R > (b)) reg_1q_pair<Real, R, (a), (b)>(v, m, u); \
+    break;
+  switch (j1 * 8 + j2) {
+    AB_PR(0, 1) AB_PR(0, 2) AB_PR(0, 3) AB_PR(0, 4) AB_PR(1, 0) AB_PR(1, 2) AB_PR(1, 3) AB_PR(1, 4)
+    AB_PR(2, 0) AB_PR(2, 1) AB_PR(2, 3) AB_PR(2, 4) AB_PR(3, 0) AB_PR(3, 1) AB_PR(3, 2) AB_PR(3, 4)
+    AB_PR(4, 0) AB_PR(4, 1) AB_PR(4, 2) AB_PR(4, 3)
+  }
+#undef AB_PR
 }
 
 template <typename Real, int R>
@@ -308,8 +369,26 @@ __global__ void __launch_bounds__(128, OCC) tile_kernel(V2<Real>* __restrict__ a
     const bool thr = (gl & op.ctrl) == op.ctrl;
     switch (op.type) {
       case OP_1Q:
-        if (op.a < 5) lane_1q<Real, R>(v, op.a, m, thr, op.creg);
-        else dispatch_reg<Real, R>(op, v, m, thr);
+        if (op.a < 5) {
+          lane_1q<Real, R>(v, op.a, m, thr, op.creg);
+          break;
+        }
+        // gate pairs need the coefficients of both gates and a quartet of
+        // temporaries live: only in the variants whose register budget
+        // (65536 / (128 * OCC), at most 255) leaves room for them beside the
+        // tile's amplitudes
+        constexpr int kBudget = 65536 / (128 * OCC) > 255 ? 255 : 65536 / (128 * OCC);
+        constexpr int kData = (1 << R) * 2 * (int)sizeof(Real) / 4;
+        constexpr bool kPairs = R >= 2 && kBudget - kData >= 96;
+        if (kPairs && op.ctrl == 0 && op.creg == 0 && i + 1 < p.op_count) {
+          const Op nx = ops[p.op_begin + i + 1];
+          if (nx.type == OP_1Q && nx.a >= 5 && nx.a != op.a && nx.ctrl == 0 && nx.creg == 0) {
+            dispatch_pair<Real, R>(op.a - 5, nx.a - 5, v, m, coef + nx.coef);
+            ++i;
+            break;
+          }
+        }
+        dispatch_reg<Real, R>(op, v, m, thr);
         break;
       case OP_X:
         if (op.a < 5) lane_x<Real, R>(v, op.a, thr, op.creg);

@@ -929,6 +929,7 @@ std::vector<std::vector<uint8_t>> split_into_involutions(const std::vector<uint3
 }
 
 int build_plan(const std::vector<Lowered>& ops, uint32_t n, const PlanOptions& o, Plan* P) {
+  P->renormalize = o.renormalize;
   std::vector<const Lowered*> seg;
   int status = ALEPH_B200_OK;
   auto flush = [&]() {

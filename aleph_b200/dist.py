@@ -324,6 +324,10 @@ class EngineRanks:
 
         self.be, self.layout, self.ranks = backend, layout, list(ranks)
         self.states = {}
+        if getattr(backend, "precision", "") == "tc32":
+            # a slice's norm is not 1: no end-of-stream rescale (as for the
+            # tile groups of an out-of-core run)
+            backend.set_tuning("renormalize", 0)
         self._torch = torch
         self.device = torch.device("cuda", torch.cuda.current_device())
         backend.synchronize()
@@ -350,6 +354,14 @@ class EngineRanks:
 
     def statevector(self, r: int) -> np.ndarray:
         return self.be.statevector(self.states[r])
+
+    def scale(self, r: int, factor: float) -> None:
+        self.be.scale_state(self.states[r], factor)
+
+    def renormalizes(self) -> bool:
+        """TC32 slices run without the end-of-stream rescale; the run restores
+        the global norm once at its end instead."""
+        return getattr(self.be, "precision", "") == "tc32"
 
     def norm_sqr(self, r: int) -> float:
         return self.be.norm_sqr(self.states[r])
@@ -466,7 +478,15 @@ def execute(plan: DistPlan, ranks, exchange: Exchange, stream_ctx: Callable | No
         else:
             exchange.run(ranks, layout, step.global_qubit, stream_ctx)
             n_ex += 1
-    return DistState(plan, ranks, exchange.world, exchange.proc, {"exchanges": n_ex, "steps": len(plan.steps)})
+    state = DistState(plan, ranks, exchange.world, exchange.proc, {"exchanges": n_ex, "steps": len(plan.steps)})
+    if getattr(ranks, "renormalizes", lambda: False)():
+        # the single-node TC32 stream ends with a rescale to norm 1; over
+        # ranks the norm is the sum of the slices' norms
+        total = norm_sqr(state)
+        if total > 0.0:
+            for r in ranks.ranks:
+                ranks.scale(r, 1.0 / np.sqrt(total))
+    return state
 
 
 def run_distributed(circuit: C.Circuit, g: int, backend, world: int = 1, rank: int = 0,

@@ -329,6 +329,12 @@ int aleph_b200_set_amplitudes(aleph_b200_handle* h, aleph_b200_state* st, const 
  * crates/aleph-cuda/src/dist/mod.rs:49-62). */
 int aleph_b200_state_memory(aleph_b200_handle* h, aleph_b200_state* st, void** device_ptr, uint64_t* bytes);
 
+/* Every amplitude times a real factor > 0, on the device. The distributed
+ * layer restores the global norm of a TC32 state held as rank slices (each
+ * slice runs without the end-of-stream renormalisation) by scaling every
+ * slice by 1 / sqrt(sum of the slices' norms). */
+int aleph_b200_scale_state(aleph_b200_handle* h, aleph_b200_state* st, double factor);
+
 /* ---- Gate::matrix (crates/aleph-core/src/gate/kinds.rs:213-400) ----
  * The dense matrix of one gate record (dim 2, 4 or 8, row-major, interleaved
  * re/im, MSB-first operand order) into out[2 * dim * dim]; UnitaryKq records
@@ -356,7 +362,12 @@ int aleph_b200_last_error_info(const aleph_b200_handle* h, aleph_b200_error_info
  * than smem_max_n relabels qubits instead of moving data, and one or two
  * in-place permutation passes settle the labels at the end of the stream),
  * "paged_local_qubits" (0..40, default 0: the most qubits one device tile
- * group of an out-of-core run may hold; 0 lets free device memory decide). */
+ * group of an out-of-core run may hold; 0 lets free device memory decide),
+ * "tile_occupancy" (0 or 2..4: the tile kernel variant, resident 128-thread
+ * blocks per SM), "tensor_blocks" (TC32 handles, 0/1), "block_window_search"
+ * (0/1), "renormalize" (0/1, default 1: a TC32 gate stream with tensor-core
+ * blocks rescales the state to norm 1 at its end; 0 for states that are one
+ * slice of a larger state, whose norm is not 1). */
 int aleph_b200_set_tuning(aleph_b200_handle* h, const char* key, int64_t value);
 
 /* ---- per-pass timing records (training data of the learned fusion planner) ---- */
