@@ -486,6 +486,7 @@ def execute(plan: DistPlan, ranks, exchange: Exchange, stream_ctx: Callable | No
         if total > 0.0:
             for r in ranks.ranks:
                 ranks.scale(r, 1.0 / np.sqrt(total))
+        ranks.be.set_tuning("renormalize", 1)  # the handle's own streams rescale again
     return state
 
 

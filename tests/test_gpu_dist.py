@@ -62,3 +62,17 @@ def test_sharded_large_slices_chunked_exchange():
     got, norm, ex = sharded(c, 2, chunk=4 << 20)
     assert ex > 0
     assert np.abs(got - want).max() <= 1e-12
+
+
+def test_handle_renormalises_again_after_a_sharded_tc32_run():
+    be = B200SvBackend(seed=0, precision="tc32")
+    st = dist.run_distributed(workloads.brickwall(14, 6, seed=97), 1, be)
+    st.ranks.free()
+    c = workloads.brickwall(16, 20, seed=98)
+    s = be.allocate(16)
+    be.apply_stream(s, c.instructions)
+    # the end-of-stream rescale ran: FP32 rounding only (a TC32 stream without
+    # it drifts by about 1e-6 per block pass)
+    assert abs(be.norm_sqr(s) - 1.0) <= 1e-6
+    s.free()
+    be.close()
