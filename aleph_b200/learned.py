@@ -275,6 +275,40 @@ def collect(backend: B200SvBackend, circuits, choices=None, repeats: int = 1):
     return np.array(X, np.float32), np.array(y, np.float32)
 
 
+def circuit_work(n: int, instr) -> float:
+    """Relative collection cost of a circuit: amplitudes x instructions."""
+    return float(1 << n) * max(1, len(instr) if not isinstance(instr, Flat) else instr.n)
+
+
+def shard_circuits(circuits, rank: int = 0, world: int = 1):
+    """This rank's share of the training circuits, for collection on several
+    GPUs. The circuits are independent units with no exchange between GPUs:
+    largest first, each goes to the rank with the least work so far
+    (amplitudes x instructions). Every rank computes the same assignment."""
+    w = [circuit_work(n, instr) for n, instr in circuits]
+    load = [0.0] * world
+    mine = []
+    for i in sorted(range(len(circuits)), key=lambda i: (-w[i], i)):
+        r = min(range(world), key=lambda k: (load[k], k))
+        load[r] += w[i]
+        if r == rank:
+            mine.append(i)
+    return [circuits[i] for i in sorted(mine)]
+
+
+def gather_samples(X: np.ndarray, y: np.ndarray, world: int = 1):
+    """Every rank's (features, targets), concatenated in rank order on every
+    rank (an all-gather of Python objects over the default process group)."""
+    if world == 1:
+        return X, y
+    import torch.distributed as dist
+
+    parts = [None] * world
+    dist.all_gather_object(parts, (X, y))
+    return (np.concatenate([p[0] for p in parts if len(p[1])]).astype(np.float32),
+            np.concatenate([p[1] for p in parts if len(p[1])]).astype(np.float32))
+
+
 TOLERANCE = {"f64": 1e-12, "f32": 1e-5, "tc32": 1e-5}
 
 
@@ -432,24 +466,43 @@ def main(argv=None) -> int:
     if args.eval_only:
         print(json.dumps({"model": str(args.out), "heldout": evaluate(args.out, **hk)}))
         return 0
+    # under torchrun every rank (one per GPU) collects its share of the
+    # circuits; rank 0 trains and evaluates on the gathered samples
+    import os
+
+    world, rank = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=3600))
     t0 = time.perf_counter()
     Xs, ys = [], []
     circuits = training_circuits(tuple(int(x) for x in args.sizes.split(",")))
     n_large = 0
     for prec in ("f64", "f32", "tc32"):
         be = B200SvBackend(seed=0, precision=prec)
-        X, y = collect(be, circuits)
+        X, y = collect(be, shard_circuits(circuits, rank, world))
         Xs.append(X)
         ys.append(y)
         if not args.no_large:
             big = large_training_circuits(prec)
-            X, y = collect(be, big, large_choices(prec))
+            X, y = collect(be, shard_circuits(big, rank, world), large_choices(prec))
             Xs.append(X)
             ys.append(y)
             n_large += len(y)
         be.close()
-    X, y = np.concatenate(Xs), np.concatenate(ys)
+    X, y = gather_samples(np.concatenate(Xs), np.concatenate(ys), world)
     t_collect = time.perf_counter() - t0
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+        if rank != 0:
+            return 0
     be = B200SvBackend(seed=0, precision="f64")
     model = CostModel(be, seed=0)
     # hold out every 10th sample to report the fit

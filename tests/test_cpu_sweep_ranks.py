@@ -79,3 +79,52 @@ def test_two_ranks_gather_the_single_rank_vector(tmp_path):
     assert sorted(l["rank"] for l in lines) == [0, 1]
     for l in lines:
         assert l["full"] == l["alone"]  # identical doubles: same evaluation, gathered
+
+
+# ---- the learned planner's training-data collection, split across ranks ----------------
+def test_training_circuits_shard_covers_every_circuit_once():
+    from aleph_b200 import learned
+
+    circuits = learned.training_circuits()
+    for world in (1, 2, 3, 8):
+        parts = [learned.shard_circuits(circuits, r, world) for r in range(world)]
+        ids = sorted(id(c) for p in parts for c in p)
+        assert ids == sorted(id(c) for c in circuits)
+        loads = [sum(learned.circuit_work(n, i) for n, i in p) for p in parts]
+        biggest = max(learned.circuit_work(n, i) for n, i in circuits)
+        assert max(loads) - min(loads) <= biggest  # largest-first, least-loaded rank
+
+
+COLLECT_SCRIPT = """
+import json, sys
+sys.path.insert(0, {root!r})
+import numpy as np
+import torch.distributed as dist
+from aleph_b200 import learned
+
+dist.init_process_group("gloo")
+rank, world = dist.get_rank(), dist.get_world_size()
+circuits = learned.training_circuits(sizes=(10, 12))
+mine = learned.shard_circuits(circuits, rank, world)
+# stand-in for the per-pass samples a GPU run records: one row per circuit
+X = np.array([[n, len(i)] for n, i in mine], np.float32).reshape(-1, 2)
+y = np.array([float(n * 1000 + len(i)) for n, i in mine], np.float32)
+Xa, ya = learned.gather_samples(X, y, world)
+print(json.dumps({{"rank": rank, "y": sorted(ya.tolist()), "rows": int(Xa.shape[0])}}), flush=True)
+dist.destroy_process_group()
+"""
+
+
+def test_training_samples_gather_over_two_ranks(tmp_path):
+    from aleph_b200 import learned
+
+    script = tmp_path / "collect_probe.py"
+    script.write_text(COLLECT_SCRIPT.format(root=str(ROOT)))
+    res = torchrun([str(script)])
+    assert res.returncode == 0, res.stderr[-2000:]
+    dec = json.JSONDecoder()
+    lines = [dec.raw_decode(res.stdout, m.start())[0] for m in re.finditer(r"\{\"rank\"", res.stdout)]
+    assert sorted(l["rank"] for l in lines) == [0, 1]
+    want = sorted(float(n * 1000 + len(i)) for n, i in learned.training_circuits(sizes=(10, 12)))
+    for l in lines:
+        assert l["y"] == want and l["rows"] == len(want)
