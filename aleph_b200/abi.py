@@ -175,6 +175,7 @@ class PlanConfig(ct.Structure):
         ("block_window_search", ct.c_uint32),
         ("tile_occupancy", ct.c_uint32),
         ("keep_swaps", ct.c_uint32),
+        ("no_pair_fusion", ct.c_uint32),
     ]
 
 

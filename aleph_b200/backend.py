@@ -412,12 +412,12 @@ class CompiledPlan:
 
 def describe_plan(num_qubits: int, instructions, precision: str = "f64", tile_r: int = 5, smem_max_n: int = 12,
                   block_window_search: bool = True, tile_occupancy: int = 0,
-                  relabel_swaps: bool = True) -> list[dict]:
+                  relabel_swaps: bool = True, pair_fusion: bool = True) -> list[dict]:
     """The passes the planner makes of ``instructions`` (host only, no device)."""
     lib = abi.load_library()
     flat = instructions if isinstance(instructions, Flat) else flatten(instructions)
     cfg = abi.PlanConfig(abi.PRECISION[precision], tile_r, smem_max_n, int(bool(block_window_search)), tile_occupancy,
-                         int(not relabel_swaps))
+                         int(not relabel_swaps), int(not pair_fusion))
     n = ct.c_uint64()
     st = lib.aleph_b200_describe_plan(num_qubits, ct.byref(cfg), flat.instrs, flat.n, ct.byref(flat.pools), None, 0,
                                       ct.byref(n))

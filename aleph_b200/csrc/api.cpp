@@ -304,7 +304,8 @@ int execute(aleph_b200_handle* h, aleph_b200_state* st, const Plan& P, const dou
         h->stats.algorithmic_bytes += 2 * len * bpa;
         break;
       case PASS_PERMUTE:
-        e = launch_permute_pass(st->amps, st->precision, st->n, ps.sigma, h->sm_count, h->stream);
+        e = launch_permute_pass(st->amps, st->precision, st->n, ps.sigma, h->sm_count, h->opts.permute_run_bits,
+                                h->stream);
         h->stats.passes++;
         h->stats.algorithmic_bytes += 2 * len * bpa;
         break;
@@ -1922,6 +1923,16 @@ int aleph_b200_set_tuning(aleph_b200_handle* h, const char* key, int64_t value) 
     h->opts.renormalize = value != 0;
     return ALEPH_B200_OK;
   }
+  if (!std::strcmp(key, "permute_run_bits")) {
+    if (value != 0 && value != 5 && value != 6)
+      return set_error(h, ALEPH_B200_INVALID_ARGUMENT, "permute_run_bits is 0, 5 or 6");
+    h->opts.permute_run_bits = (uint32_t)value;
+    return ALEPH_B200_OK;
+  }
+  if (!std::strcmp(key, "pair_fusion")) {
+    h->opts.pair_fusion = value != 0;
+    return ALEPH_B200_OK;
+  }
   if (!std::strcmp(key, "tensor_blocks")) {
     if (h->precision != ALEPH_B200_TC32)
       return set_error(h, ALEPH_B200_INVALID_ARGUMENT, "tensor_blocks applies to TC32 handles only");
@@ -1965,6 +1976,7 @@ int aleph_b200_describe_plan(uint32_t num_qubits, const aleph_b200_plan_config* 
   tmp.opts.block_window_search = config->block_window_search != 0;
   tmp.opts.tile_occupancy = config->tile_occupancy;
   tmp.opts.relabel_swaps = config->keep_swaps == 0;
+  tmp.opts.pair_fusion = config->no_pair_fusion == 0;
   std::vector<Lowered> ops;
   if (int r = lower_stream(&tmp, num_qubits, in, count, pools, &ops)) return r;
   Plan P;

@@ -222,25 +222,26 @@ cudaError_t launch_convert(const void* src, int sp, void* dst, int dp, uint64_t 
 // permuted local index stay conflict-free.
 namespace perm {
 
-constexpr int THREADS = 256;
-constexpr int MAX_TILE_BITS = 10;
-constexpr int MAX_TILE = 1 << MAX_TILE_BITS;
-constexpr int PER_THREAD = MAX_TILE / THREADS;
-
+// A tile is 2^tile_bits amplitudes: qubits 0..RB-1 (runs of 2^RB contiguous
+// amplitudes), their images under sigma, then fixed points and transposed
+// pairs up to 2*RB bits. RB = 6 (1 KiB FP64 runs, 4096-amplitude tiles) for
+// n >= 12; RB = 5 below. Local index o = column (bits 0..RB-1) | row << RB.
+template <int RB>
 struct Geometry {
+  static constexpr int W = 1 << RB;
   uint32_t tile_bits;                 // |T|
   uint32_t n_outer;                   // |O|
   uint32_t local_identity;            // sigma fixes every tile bit: self-mapped tiles stay put
   uint8_t ob[kMaxQubits];             // outer positions, ascending
   uint8_t osig[kMaxQubits];           // index in ob of sigma(ob[m])
-  uint64_t dep_hi[32];                // global offset of local bits 5.. (indexed by local >> 5)
-  uint16_t sig_lo[32], sig_hi[32];    // local sigma: sig_lo[local & 31] ^ sig_hi[local >> 5]
+  uint64_t dep_hi[W];                 // global offset of a row's local bits
+  // shared-memory slots: a tile amplitude o sits at slot o ^ wr_hi[row(o)]
+  // (a per-row XOR of the column), and the amplitude that replaces it comes
+  // from slot rd_lo[col(o)] ^ rd_hi[row(o)] (the swizzled slot of sigma(o))
+  uint16_t wr_hi[W], rd_lo[W], rd_hi[W];
 };
 
-__device__ __forceinline__ uint32_t swz(uint32_t o) { return o ^ ((o >> 5) & 31u); }
-
-// The CTA's work items: outer values h (grid-stride) that own a pair or a
-// self-mapped tile that moves. Uniform across the CTA.
+// Work item: an outer value h that owns a pair, or a self-mapped tile that moves.
 struct Item {
   uint64_t h, b1, b2;
   bool pair;
@@ -260,23 +261,30 @@ __device__ __forceinline__ uint64_t or_across_warp(uint64_t x) {
 }
 
 // Every warp decodes h with one lane per outer bit (no per-thread bit loop).
-__device__ __forceinline__ Item next_item(const Geometry& g, const LaneBit& lb, uint64_t h, uint64_t nh) {
+__device__ __forceinline__ Item next_item(uint32_t local_identity, const LaneBit& lb, uint64_t h, uint64_t nh) {
   for (; h < nh; h += gridDim.x) {
     const uint64_t bit = lb.act ? (h >> lb.m) & 1ull : 0ull;
     const uint64_t h2 = or_across_warp(bit << lb.to_h2);
-    if (h2 < h) continue;                     // the pair belongs to its smaller member
-    if (h2 == h && g.local_identity) continue;  // a fixed tile: nothing moves
+    if (h2 < h) continue;                   // the pair belongs to its smaller member
+    if (h2 == h && local_identity) continue;  // a fixed tile: nothing moves
     return Item{h, or_across_warp(bit << lb.to_b1), or_across_warp(bit << lb.to_b2), h2 != h};
   }
   return Item{nh, 0, 0, false};
 }
 
 // Software pipeline: the next item's loads are issued once the current item
-// sits in shared memory, and are in flight during its write-back.
-template <typename Real>
-__global__ void __launch_bounds__(THREADS) permute_kernel(V2<Real>* __restrict__ X, const Geometry g) {
-  __shared__ V2<Real> S1[MAX_TILE], S2[MAX_TILE];
+// sits in shared memory, and are in flight during its write-back. Each thread
+// owns one column (o & (W-1) is fixed, THREADS is a multiple of W), so rows
+// are warp-uniform: the row tables are uniform parameter reads.
+template <typename Real, int RB, int THREADS, int MINB>
+__global__ void __launch_bounds__(THREADS, MINB) permute_kernel(V2<Real>* __restrict__ X, const Geometry<RB> g) {
+  constexpr uint32_t W = 1u << RB;
+  constexpr int PER_THREAD = (1 << (2 * RB)) / THREADS;
+  constexpr uint32_t ROWS_PER_STEP = THREADS / W;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  V2<Real>* S1 = reinterpret_cast<V2<Real>*>(smem_raw);
   const uint32_t T = 1u << g.tile_bits;
+  V2<Real>* S2 = S1 + T;
   const uint64_t nh = 1ull << g.n_outer;
   // lane-indexed parameters are read once (a lane-divergent read of the
   // parameter bank serialises across the warp)
@@ -287,41 +295,44 @@ __global__ void __launch_bounds__(THREADS) permute_kernel(V2<Real>* __restrict__
   lb.to_h2 = lb.act ? g.osig[lane] : 0u;
   lb.to_b1 = lb.act ? g.ob[lane] : 0u;
   lb.to_b2 = lb.act ? g.ob[g.osig[lane]] : 0u;
-  const uint32_t sig_lane = g.sig_lo[lane];  // local bits 0..4 of o are the lane
+  const uint32_t col = threadIdx.x & (W - 1u);
+  const uint32_t row0 = threadIdx.x / W;
+  const uint32_t rd_col = g.rd_lo[col];
   V2<Real> r1[PER_THREAD], r2[PER_THREAD];
   auto load = [&](const Item& it) {
 #pragma unroll
     for (int k = 0; k < PER_THREAD; ++k) {
-      const uint32_t o = threadIdx.x + (uint32_t)k * THREADS;
-      if (o < T) {
-        const uint64_t off = (o & 31u) | g.dep_hi[o >> 5];
+      const uint32_t row = row0 + (uint32_t)k * ROWS_PER_STEP;
+      if (((row << RB) | col) < T) {
+        const uint64_t off = col | g.dep_hi[row];
         r1[k] = X[it.b1 + off];
         if (it.pair) r2[k] = X[it.b2 + off];
       }
     }
   };
-  Item cur = next_item(g, lb, blockIdx.x, nh);
+  Item cur = next_item(g.local_identity, lb, blockIdx.x, nh);
   if (cur.h >= nh) return;
   load(cur);
   for (;;) {
     __syncthreads();  // the previous write-back is done reading shared memory
 #pragma unroll
     for (int k = 0; k < PER_THREAD; ++k) {
-      const uint32_t o = threadIdx.x + (uint32_t)k * THREADS;
-      if (o < T) {
-        S1[swz(o)] = r1[k];
-        if (cur.pair) S2[swz(o)] = r2[k];
+      const uint32_t row = row0 + (uint32_t)k * ROWS_PER_STEP;
+      if (((row << RB) | col) < T) {
+        const uint32_t slot = (row << RB) | (col ^ g.wr_hi[row]);
+        S1[slot] = r1[k];
+        if (cur.pair) S2[slot] = r2[k];
       }
     }
     __syncthreads();
-    const Item nxt = next_item(g, lb, cur.h + gridDim.x, nh);
+    const Item nxt = next_item(g.local_identity, lb, cur.h + gridDim.x, nh);
     if (nxt.h < nh) load(nxt);
 #pragma unroll
     for (int k = 0; k < PER_THREAD; ++k) {
-      const uint32_t o = threadIdx.x + (uint32_t)k * THREADS;
-      if (o < T) {
-        const uint32_t s = swz(sig_lane ^ (uint32_t)g.sig_hi[o >> 5]);
-        const uint64_t off = (o & 31u) | g.dep_hi[o >> 5];
+      const uint32_t row = row0 + (uint32_t)k * ROWS_PER_STEP;
+      if (((row << RB) | col) < T) {
+        const uint32_t s = rd_col ^ g.rd_hi[row];
+        const uint64_t off = col | g.dep_hi[row];
         X[cur.b1 + off] = cur.pair ? S2[s] : S1[s];
         if (cur.pair) X[cur.b2 + off] = S1[s];
       }
@@ -331,12 +342,17 @@ __global__ void __launch_bounds__(THREADS) permute_kernel(V2<Real>* __restrict__
   }
 }
 
-// Tile geometry of an involution (host side).
-static Geometry geometry(uint32_t n, const uint8_t* sigma) {
-  Geometry g;
+// Tile geometry of an involution (host side). `bank_bits`: the column bits
+// whose lanes share one shared-memory wavefront (3 for 16-byte amplitudes,
+// 4 for 8-byte ones); the row swizzle sends the rows that those lanes read
+// after sigma to distinct bank groups.
+template <int RB>
+static Geometry<RB> geometry(uint32_t n, const uint8_t* sigma, uint32_t bank_bits) {
+  constexpr uint32_t W = 1u << RB;
+  Geometry<RB> g;
   std::memset(&g, 0, sizeof(g));
-  const uint32_t nl = n < 5 ? n : 5;
-  const uint32_t want = n < (uint32_t)MAX_TILE_BITS ? n : (uint32_t)MAX_TILE_BITS;
+  const uint32_t nl = n < (uint32_t)RB ? n : (uint32_t)RB;
+  const uint32_t want = n < 2u * RB ? n : 2u * RB;
   uint64_t T = 0;
   for (uint32_t q = 0; q < nl; ++q) T |= (1ull << q) | (1ull << sigma[q]);
   auto count = [&]() { return (uint32_t)__builtin_popcountll(T); };
@@ -360,49 +376,89 @@ static Geometry geometry(uint32_t n, const uint8_t* sigma) {
   g.local_identity = 1;
   for (uint32_t j = 0; j < k; ++j) g.local_identity &= sigma[tb[j]] == tb[j] ? 1u : 0u;
   for (uint32_t j = 0; j < m; ++j) g.osig[j] = outer_of[sigma[g.ob[j]]];
-  for (uint32_t x = 0; x < 32; ++x) {
-    uint32_t lo = 0, hi = 0;
+  // local sigma as a bit map of the tile index
+  uint32_t lsig[2 * RB] = {};
+  for (uint32_t j = 0; j < k; ++j) lsig[j] = local_of[sigma[tb[j]]];
+  // row swizzle: a linear map M from row bits to column bits. Lane bit b < bank_bits
+  // (a column bit) reads local bit lsig[b]; when that is a row bit, M sends it to
+  // a bank bit not yet taken, so the 2^bank_bits lanes of a wavefront hit
+  // distinct bank groups.
+  uint32_t Mrow[RB] = {};
+  uint32_t used = 0;
+  for (uint32_t b = 0; b < bank_bits && b < k; ++b)
+    if (lsig[b] < (uint32_t)RB && lsig[b] < bank_bits) used |= 1u << lsig[b];
+  for (uint32_t b = 0; b < bank_bits && b < k; ++b) {
+    if (lsig[b] < (uint32_t)RB) continue;
+    uint32_t free_bit = 0;
+    while (free_bit < bank_bits && ((used >> free_bit) & 1)) ++free_bit;
+    if (free_bit == bank_bits) break;
+    Mrow[lsig[b] - RB] = 1u << free_bit;
+    used |= 1u << free_bit;
+  }
+  auto M = [&](uint32_t row) {
+    uint32_t x = 0;
+    for (uint32_t r = 0; r < (uint32_t)RB; ++r)
+      if ((row >> r) & 1) x ^= Mrow[r];
+    return x;
+  };
+  auto sig_local = [&](uint32_t o) {
+    uint32_t x = 0;
+    for (uint32_t j = 0; j < k; ++j)
+      if ((o >> j) & 1) x |= 1u << lsig[j];
+    return x;
+  };
+  auto slot = [&](uint32_t o) { return o ^ M(o >> RB); };
+  for (uint32_t x = 0; x < W; ++x) {
     uint64_t dep = 0;
-    for (uint32_t b = 0; b < 5; ++b) {
-      if (!((x >> b) & 1)) continue;
-      if (b < k) lo |= 1u << local_of[sigma[tb[b]]];
-      if (5 + b < k) {
-        hi |= 1u << local_of[sigma[tb[5 + b]]];
-        dep |= 1ull << tb[5 + b];
-      }
-    }
-    g.sig_lo[x] = (uint16_t)lo;
-    g.sig_hi[x] = (uint16_t)hi;
+    for (uint32_t b = 0; b < (uint32_t)RB; ++b)
+      if (((x >> b) & 1) && RB + b < k) dep |= 1ull << tb[RB + b];
     g.dep_hi[x] = dep;
+    g.wr_hi[x] = (uint16_t)M(x);
+    // slot(sig(o)) is linear in o: split into its column and row parts
+    g.rd_lo[x] = (uint16_t)(x < (1u << k) ? slot(sig_local(x)) : 0u);
+    g.rd_hi[x] = (uint16_t)((x << RB) < (1u << k) ? slot(sig_local(x << RB)) : 0u);
   }
   return g;
+}
+
+template <typename Real, int RB, int THREADS, int MINB>
+static cudaError_t launch_rb(void* amps, uint32_t n, const uint8_t* sigma, int sm_count, cudaStream_t s) {
+  const uint32_t bank_bits = sizeof(V2<Real>) == 16 ? 3u : 4u;
+  const Geometry<RB> g = geometry<RB>(n, sigma, bank_bits);
+  if (g.n_outer > 31) return cudaErrorInvalidValue;  // one lane per outer bit
+  const uint64_t nh = 1ull << g.n_outer;
+  const size_t shm = 2 * ((size_t)1 << g.tile_bits) * sizeof(V2<Real>);
+  constexpr size_t kMaxShm = 2 * ((size_t)1 << (2 * RB)) * sizeof(V2<Real>);
+  auto kern = permute_kernel<Real, RB, THREADS, MINB>;
+  // a persistent grid: exactly the CTAs that are resident at once
+  static int resident = 0;
+  if (!resident) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxShm);
+    if (e != cudaSuccess) return e;
+    int nb = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, THREADS, kMaxShm);
+    if (e != cudaSuccess) return e;
+    resident = nb > 0 ? nb : 1;
+  }
+  const uint64_t want = (uint64_t)(sm_count > 0 ? sm_count : 148) * (uint64_t)resident;
+  const unsigned blocks = (unsigned)(nh < want ? nh : want);
+  kern<<<blocks, THREADS, shm, s>>>((V2<Real>*)amps, g);
+  return cudaGetLastError();
 }
 
 }  // namespace perm
 
 cudaError_t launch_permute_pass(void* amps, int precision, uint32_t n, const uint8_t* sigma, int sm_count,
-                                cudaStream_t s) {
-  const perm::Geometry g = perm::geometry(n, sigma);
-  if (g.n_outer > 31) return cudaErrorInvalidValue;  // one lane per outer bit
-  const uint64_t nh = 1ull << g.n_outer;
-  // a persistent grid: exactly the CTAs that are resident at once
-  static int resident[2] = {0, 0};
-  const int k = precision == ALEPH_B200_F64 ? 1 : 0;
-  if (!resident[k]) {
-    int nb = 0;
-    const cudaError_t e =
-        k ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, perm::permute_kernel<double>, perm::THREADS, 0)
-          : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, perm::permute_kernel<float>, perm::THREADS, 0);
-    if (e != cudaSuccess) return e;
-    resident[k] = nb > 0 ? nb : 1;
-  }
-  const uint64_t want = (uint64_t)(sm_count > 0 ? sm_count : 148) * (uint64_t)resident[k];
-  const unsigned blocks = (unsigned)(nh < want ? nh : want);
-  if (k)
-    perm::permute_kernel<double><<<blocks, perm::THREADS, 0, s>>>((double2*)amps, g);
-  else
-    perm::permute_kernel<float><<<blocks, perm::THREADS, 0, s>>>((float2*)amps, g);
-  return cudaGetLastError();
+                                uint32_t run_bits, cudaStream_t s) {
+  // 64-amplitude runs (n >= 12): 4096-amplitude tiles, a tile pair is 128 KiB
+  // of shared memory in FP64 (one CTA of 512 threads per SM), 64 KiB in FP32
+  // (two per SM). 32-amplitude runs: 1024-amplitude tiles, several CTAs per SM.
+  const bool wide = n >= 12 && run_bits == 6;
+  if (precision == ALEPH_B200_F64)
+    return wide ? perm::launch_rb<double, 6, 512, 1>(amps, n, sigma, sm_count, s)
+                : perm::launch_rb<double, 5, 256, 1>(amps, n, sigma, sm_count, s);
+  return wide ? perm::launch_rb<float, 6, 512, 2>(amps, n, sigma, sm_count, s)
+              : perm::launch_rb<float, 5, 256, 1>(amps, n, sigma, sm_count, s);
 }
 
 // ---- renormalisation (end of a tensor-core gate stream) ----------------------

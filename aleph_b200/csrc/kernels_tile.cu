@@ -368,7 +368,7 @@ __global__ void __launch_bounds__(128, OCC) tile_kernel(V2<Real>* __restrict__ a
     const V2<Real>* m = coef + op.coef;
     const bool thr = (gl & op.ctrl) == op.ctrl;
     switch (op.type) {
-      case OP_1Q:
+      case OP_1Q: {
         if (op.a < 5) {
           lane_1q<Real, R>(v, op.a, m, thr, op.creg);
           break;
@@ -390,6 +390,7 @@ __global__ void __launch_bounds__(128, OCC) tile_kernel(V2<Real>* __restrict__ a
         }
         dispatch_reg<Real, R>(op, v, m, thr);
         break;
+      }
       case OP_X:
         if (op.a < 5) lane_x<Real, R>(v, op.a, thr, op.creg);
         else dispatch_reg<Real, R>(op, v, m, thr);

@@ -17,6 +17,7 @@
 // gates run in registers one after the other.
 
 #include <algorithm>
+#include <deque>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -517,6 +518,178 @@ void swap_2q_operands(std::vector<double>& c) {
   c = out;
 }
 
+// ---- pair fusion (warp-tile passes) ------------------------------------------
+// A tile pass applies its gates one at a time in registers, so its arithmetic
+// is the sum of the gates': 8 FP64 multiply-adds per amplitude for a dense
+// one-qubit gate, 16 for a dense two-qubit one, one or two for a diagonal.
+// In FP64 the pass is bound by that arithmetic. A two-qubit gate together
+// with the one-qubit gates around it on its two qubits is one 4x4 (16 per
+// amplitude): in a brickwall, the one-qubit layers on both sides of a CZ,
+// four dense gates (32) for one 4x4 (16).
+//
+// The rule, in gate order: one-qubit gates wait on their qubit. A gate on
+// exactly two qubits a, b opens a block that takes the waiting one-qubit
+// gates of a and b, itself, then every later gate on a and/or b alone, until
+// a gate touches a or b together with another qubit. The block is then
+// emitted as one 4x4 when its gates cost at least 24 per amplitude; otherwise
+// its gates are emitted unchanged and the one-qubit gates at its end wait
+// again on their qubits (so a CZ between two already-absorbed layers leaves
+// the next layer to the next block). This is the idea of Fuse2q
+// (crates/aleph-ir/src/passes/fuse_2q.rs) with a cost rule for register tiles.
+void apply_local(const Lowered& L, const uint32_t* bq, Cx* s);
+
+namespace {
+
+int tile_cost(const Lowered& L) {
+  switch (L.op.type) {
+    case OP_1Q: return 8;
+    case OP_2Q: return 16;
+    case OP_X: case OP_NEG: return 1;
+    case OP_CPHASE: case OP_DIAG: return 2;
+    default: return 32;
+  }
+}
+
+constexpr int kFuseMinCost = 24;
+
+// The 4x4 of an op on qubits {a (matrix MSB), b (LSB)}, right-multiplied into m:
+// m := op * m.
+void fold_into_4x4(const Lowered& L, uint32_t a, uint32_t b, Cx* m) {
+  const uint32_t bq[6] = {b, a, 60, 61, 62, 63};  // local bit 0 = b, bit 1 = a
+  Cx out[16];
+  for (uint32_t c = 0; c < 4; ++c) {
+    Cx s[64];
+    for (auto& x : s) x = Cx{0, 0};
+    for (uint32_t r = 0; r < 4; ++r) s[r] = m[r * 4 + c];
+    apply_local(L, bq, s);
+    for (uint32_t r = 0; r < 4; ++r) out[r * 4 + c] = s[r];
+  }
+  for (int i = 0; i < 16; ++i) m[i] = out[i];
+}
+
+bool fusable_type(const Lowered& L) {
+  return !L.is_measure && !L.is_permute && L.op.type != OP_POLY && L.op.type != OP_KQ;
+}
+
+}  // namespace
+
+std::vector<const Lowered*> fuse_pairs(const std::vector<const Lowered*>& seg, std::deque<Lowered>& store) {
+  struct Block {
+    uint32_t a, b;
+    Cx m[16];
+    std::vector<const Lowered*> members;
+    int cost = 0;
+    uint32_t record = 0;
+  };
+  std::vector<const Lowered*> out;
+  out.reserve(seg.size());
+  std::vector<std::vector<size_t>> waiting(kMaxQubits);  // out indices of one-qubit gates waiting per qubit
+  std::vector<int> open(kMaxQubits, -1);
+  std::vector<Block> blocks;
+  auto close = [&](uint32_t q) {
+    const int k = open[q];
+    if (k < 0) return;
+    Block& B = blocks[(size_t)k];
+    open[B.a] = open[B.b] = -1;
+    if (B.cost >= kFuseMinCost) {
+      store.emplace_back();
+      Lowered& F = store.back();
+      std::memset(&F.op, 0, sizeof(Op));
+      F.op.type = OP_2Q;
+      F.op.nq = 2;
+      F.op.q[0] = (uint8_t)B.a;
+      F.op.q[1] = (uint8_t)B.b;
+      push_coef(&F, B.m, 16);
+      F.nondiag = (1ull << B.a) | (1ull << B.b);
+      F.diag = 0;
+      F.record = B.record;
+      F.gates = 0;
+      for (const Lowered* L : B.members) F.gates += L->gates ? L->gates : 1;
+      out.push_back(&F);
+      waiting[B.a].clear();
+      waiting[B.b].clear();
+      return;
+    }
+    // not worth a 4x4: the gates go out as they came; the one-qubit gates
+    // after the block's last two-qubit gate wait again on their qubits
+    size_t last2 = 0;
+    for (size_t i = 0; i < B.members.size(); ++i)
+      if (__builtin_popcountll(B.members[i]->nondiag | B.members[i]->diag) == 2) last2 = i;
+    waiting[B.a].clear();
+    waiting[B.b].clear();
+    for (size_t i = 0; i < B.members.size(); ++i) {
+      out.push_back(B.members[i]);
+      if (i > last2) {
+        const uint64_t t = B.members[i]->nondiag | B.members[i]->diag;
+        waiting[(uint32_t)__builtin_ctzll(t)].push_back(out.size() - 1);
+      }
+    }
+  };
+  for (const Lowered* L : seg) {
+    const uint64_t touched = L->nondiag | L->diag;
+    const int width = __builtin_popcountll(touched);
+    if (fusable_type(*L) && width == 1) {
+      const uint32_t q = (uint32_t)__builtin_ctzll(touched);
+      const int k = open[q];
+      if (k >= 0) {
+        Block& B = blocks[(size_t)k];
+        fold_into_4x4(*L, B.a, B.b, B.m);
+        B.members.push_back(L);
+        B.cost += tile_cost(*L);
+      } else {
+        out.push_back(L);
+        waiting[q].push_back(out.size() - 1);
+      }
+      continue;
+    }
+    if (fusable_type(*L) && width == 2) {
+      const uint32_t lo = (uint32_t)__builtin_ctzll(touched), hi = 63u - (uint32_t)__builtin_clzll(touched);
+      if (open[lo] >= 0 && open[lo] == open[hi]) {  // another gate on the same pair
+        Block& B = blocks[(size_t)open[lo]];
+        fold_into_4x4(*L, B.a, B.b, B.m);
+        B.members.push_back(L);
+        B.cost += tile_cost(*L);
+        continue;
+      }
+      close(lo);
+      close(hi);
+      Block B;
+      B.a = hi;
+      B.b = lo;
+      for (int i = 0; i < 16; ++i) B.m[i] = Cx{(i % 5) == 0 ? 1.0 : 0.0, 0.0};
+      B.record = L->record;
+      for (uint32_t q : {hi, lo}) {
+        for (size_t idx : waiting[q]) {
+          const Lowered* W = out[idx];
+          fold_into_4x4(*W, B.a, B.b, B.m);
+          B.members.push_back(W);
+          B.cost += tile_cost(*W);
+          out[idx] = nullptr;
+        }
+        waiting[q].clear();
+      }
+      fold_into_4x4(*L, B.a, B.b, B.m);
+      B.members.push_back(L);
+      B.cost += tile_cost(*L);
+      blocks.push_back(std::move(B));
+      open[hi] = open[lo] = (int)blocks.size() - 1;
+      continue;
+    }
+    for (uint32_t q = 0; q < kMaxQubits; ++q)
+      if ((touched >> q) & 1) {
+        close(q);
+        waiting[q].clear();
+      }
+    out.push_back(L);
+  }
+  for (uint32_t q = 0; q < kMaxQubits; ++q) close(q);
+  std::vector<const Lowered*> compact;
+  compact.reserve(out.size());
+  for (const Lowered* L : out)
+    if (L) compact.push_back(L);
+  return compact;
+}
+
 int plan_segment_tiles(const std::vector<const Lowered*>& seg, uint32_t n, uint32_t R, Plan* P) {
   std::vector<const Lowered*> pending = seg;
   while (!pending.empty()) {
@@ -631,7 +804,8 @@ int plan_segment_tiles(const std::vector<const Lowered*>& seg, uint32_t n, uint3
     ps.kind = PASS_TILE;
     ps.tile = tp;
     ps.record = take.empty() ? 0 : take.front()->record;
-    ps.gates = (uint32_t)take.size();
+    ps.gates = 0;
+    for (const Lowered* L : take) ps.gates += L->gates ? L->gates : 1;
     count_ops(take, &ps);
     P->passes.push_back(ps);
     pending.swap(rest);
@@ -949,7 +1123,12 @@ int build_plan(const std::vector<Lowered>& ops, uint32_t n, const PlanOptions& o
       // a 2-qubit gate may need two register qubits: R >= 2 unless only one high qubit exists
       const uint32_t R = std::min<uint32_t>(std::max<uint32_t>(o.tile_r, 2), std::min<uint32_t>(5, n - 5));
       if (o.tensor_blocks && n >= 13) status = plan_segment_blocks(seg, n, R, o.block_window_search, P);
-      else status = plan_segment_tiles(seg, n, R, P);
+      else if (o.pair_fusion) {
+        std::deque<Lowered> fused;
+        status = plan_segment_tiles(fuse_pairs(seg, fused), n, R, P);
+      } else {
+        status = plan_segment_tiles(seg, n, R, P);
+      }
     }
     seg.clear();
   };

@@ -367,7 +367,10 @@ int aleph_b200_last_error_info(const aleph_b200_handle* h, aleph_b200_error_info
  * blocks per SM), "tensor_blocks" (TC32 handles, 0/1), "block_window_search"
  * (0/1), "renormalize" (0/1, default 1: a TC32 gate stream with tensor-core
  * blocks rescales the state to norm 1 at its end; 0 for states that are one
- * slice of a larger state, whose norm is not 1). */
+ * slice of a larger state, whose norm is not 1), "pair_fusion" (0/1,
+ * default 1: in warp-tile passes a gate on two qubits and the one-qubit
+ * gates next to it on those qubits run as one 4x4 when that saves
+ * arithmetic). */
 int aleph_b200_set_tuning(aleph_b200_handle* h, const char* key, int64_t value);
 
 /* ---- per-pass timing records (training data of the learned fusion planner) ---- */
@@ -400,6 +403,7 @@ typedef struct aleph_b200_plan_config {
   uint32_t block_window_search;  /* TC32: also try every 6-qubit window      */
   uint32_t tile_occupancy;       /* tile kernel variant: 0 (default) or 2..4 */
   uint32_t keep_swaps;           /* 1: SWAP records run as gates; 0: relabel */
+  uint32_t no_pair_fusion;       /* 1: tile passes apply every gate as given */
 } aleph_b200_plan_config;
 int aleph_b200_describe_plan(uint32_t num_qubits, const aleph_b200_plan_config* config, const aleph_b200_instr* instrs,
                              uint64_t count, const aleph_b200_pools* pools, aleph_b200_pass_record* out, uint64_t cap,

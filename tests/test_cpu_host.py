@@ -247,9 +247,13 @@ def test_learned_candidates_and_features():
     assert X.shape == (len(recs), learned.N_FEATURES) and np.isfinite(X).all()
     assert (X[:, 1] == 1).all()  # every pass is a tensor-core block
     assert sum(r["dense_ops"] + r["diag_ops"] for r in recs) == c.gate_count()
-    t = describe_plan(24, c.instructions, "f64", tile_r=4, tile_occupancy=3)
+    t = describe_plan(24, c.instructions, "f64", tile_r=4, tile_occupancy=3, pair_fusion=False)
     assert all(r["variant"] == 3 and len(r["qubits"]) == 4 for r in t)
     assert sum(r["dense_ops"] + r["diag_ops"] for r in t) == c.gate_count()
+    # pair fusion: one 4x4 op stands for several gates; the pass still counts them all
+    f = describe_plan(24, c.instructions, "f64", tile_r=4, tile_occupancy=3)
+    assert sum(r["gates"] for r in f) == c.gate_count()
+    assert sum(r["dense_ops"] + r["diag_ops"] for r in f) < c.gate_count()
 
 
 def test_grover_workload_amplifies_the_marked_state():
