@@ -304,8 +304,7 @@ int execute(aleph_b200_handle* h, aleph_b200_state* st, const Plan& P, const dou
         h->stats.algorithmic_bytes += 2 * len * bpa;
         break;
       case PASS_PERMUTE:
-        e = launch_permute_pass(st->amps, st->precision, st->n, ps.sigma, h->sm_count, h->opts.permute_run_bits,
-                                h->stream);
+        e = launch_permute_pass(st->amps, st->precision, st->n, ps.sigma, h->sm_count, h->stream);
         h->stats.passes++;
         h->stats.algorithmic_bytes += 2 * len * bpa;
         break;
@@ -1921,12 +1920,6 @@ int aleph_b200_set_tuning(aleph_b200_handle* h, const char* key, int64_t value) 
   }
   if (!std::strcmp(key, "renormalize")) {
     h->opts.renormalize = value != 0;
-    return ALEPH_B200_OK;
-  }
-  if (!std::strcmp(key, "permute_run_bits")) {
-    if (value != 0 && value != 5 && value != 6)
-      return set_error(h, ALEPH_B200_INVALID_ARGUMENT, "permute_run_bits is 0, 5 or 6");
-    h->opts.permute_run_bits = (uint32_t)value;
     return ALEPH_B200_OK;
   }
   if (!std::strcmp(key, "pair_fusion")) {

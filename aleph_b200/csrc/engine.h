@@ -151,7 +151,6 @@ struct PlanOptions {
   bool relabel_swaps = true;        // SWAPs relabel qubits; one permutation pass settles the map
   bool renormalize = true;          // TC32: rescale to norm 1 after a stream's block passes
   bool pair_fusion = true;          // tile passes: a two-qubit gate and its one-qubit neighbours as one 4x4
-  uint32_t permute_run_bits = 0;    // permutation passes: 2^k-amplitude runs (5 or 6; 0 = by size and precision)
 };
 
 // ---------------------------------------------------------------------------
@@ -233,10 +232,9 @@ cudaError_t launch_renormalize(void* amps, int precision, uint32_t n, double* pa
                                cudaStream_t s);
 cudaError_t launch_convert(const void* src, int src_prec, void* dst, int dst_prec, uint64_t count, cudaStream_t s);
 // In-place qubit-permutation pass: psi(j) -> psi(sigma(j)) for an involution
-// sigma of the n qubit positions (sigma[sigma[q]] == q). run_bits: the tile's
-// contiguous run, 2^run_bits amplitudes (5 or 6; 0 picks by size and precision).
+// sigma of the n qubit positions (sigma[sigma[q]] == q).
 cudaError_t launch_permute_pass(void* amps, int precision, uint32_t n, const uint8_t* sigma, int sm_count,
-                                uint32_t run_bits, cudaStream_t s);
+                                cudaStream_t s);
 // Splits the position permutation pi (bit q of an index moves to pi[q]) into
 // involutions applied in order: psi o pi = P_last ... P_first psi, where a
 // pass P_sigma maps psi(j) -> psi(sigma(j)). At most two; none for the identity.

@@ -449,16 +449,14 @@ static cudaError_t launch_rb(void* amps, uint32_t n, const uint8_t* sigma, int s
 }  // namespace perm
 
 cudaError_t launch_permute_pass(void* amps, int precision, uint32_t n, const uint8_t* sigma, int sm_count,
-                                uint32_t run_bits, cudaStream_t s) {
-  // 64-amplitude runs (n >= 12): 4096-amplitude tiles, a tile pair is 128 KiB
-  // of shared memory in FP64 (one CTA of 512 threads per SM), 64 KiB in FP32
-  // (two per SM). 32-amplitude runs: 1024-amplitude tiles, several CTAs per SM.
-  const bool wide = n >= 12 && run_bits == 6;
-  if (precision == ALEPH_B200_F64)
-    return wide ? perm::launch_rb<double, 6, 512, 1>(amps, n, sigma, sm_count, s)
-                : perm::launch_rb<double, 5, 256, 1>(amps, n, sigma, sm_count, s);
-  return wide ? perm::launch_rb<float, 6, 512, 2>(amps, n, sigma, sm_count, s)
-              : perm::launch_rb<float, 5, 256, 1>(amps, n, sigma, sm_count, s);
+                                cudaStream_t s) {
+  // 32-amplitude runs and 1024-amplitude tiles: a tile pair is 32 KiB of
+  // shared memory in FP64, so several CTAs share an SM and cover each other's
+  // barrier bubbles. (64-amplitude runs need a 128 KiB pair, one CTA per SM:
+  // slower on B200 for every permutation measured, 2.4-3.1 against
+  // 3.7-5.5 TB/s in FP64.)
+  if (precision == ALEPH_B200_F64) return perm::launch_rb<double, 5, 256, 1>(amps, n, sigma, sm_count, s);
+  return perm::launch_rb<float, 5, 256, 1>(amps, n, sigma, sm_count, s);
 }
 
 // ---- renormalisation (end of a tensor-core gate stream) ----------------------
