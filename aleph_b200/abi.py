@@ -157,7 +157,7 @@ class PassRecord(ct.Structure):
         ("dense_ops", ct.c_uint32),
         ("diag_ops", ct.c_uint32),
         ("variant", ct.c_uint32),
-        ("pad", ct.c_uint32),
+        ("fma_per_amp", ct.c_uint32),
         ("ms", ct.c_double),
         ("bytes", ct.c_double),
     ]

@@ -377,7 +377,7 @@ class B200SvBackend:
 def _record_dict(r) -> dict:
     return {"kind": abi.PASS_KINDS.get(r.kind, r.kind), "gates": r.gates, "n": r.n, "qubits": list(r.qubits[: r.nq]),
             "post_ops": r.post_ops, "lane_ops": r.lane_ops, "dense_ops": r.dense_ops, "diag_ops": r.diag_ops,
-            "variant": r.variant, "ms": r.ms, "bytes": r.bytes}
+            "variant": r.variant, "fma_per_amp": r.fma_per_amp, "ms": r.ms, "bytes": r.bytes}
 
 
 class CompiledPlan:

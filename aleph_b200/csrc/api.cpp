@@ -323,6 +323,7 @@ int execute(aleph_b200_handle* h, aleph_b200_state* st, const Plan& P, const dou
         r.lane_ops = ps.lane_ops;
         r.dense_ops = ps.dense_ops;
         r.diag_ops = ps.diag_ops;
+        r.fma_per_amp = ps.fma_per_amp;
         r.variant = ps.kind == PASS_TILE ? ps.tile.occupancy : 0;
       }
     }
@@ -1990,6 +1991,7 @@ int aleph_b200_describe_plan(uint32_t num_qubits, const aleph_b200_plan_config* 
     r.lane_ops = ps.lane_ops;
     r.dense_ops = ps.dense_ops;
     r.diag_ops = ps.diag_ops;
+    r.fma_per_amp = ps.fma_per_amp;
     r.variant = ps.kind == PASS_TILE ? ps.tile.occupancy : 0;
     r.bytes = (ps.kind == PASS_MEASURE ? 3 : 2) * len * bpa;
     out[k] = r;

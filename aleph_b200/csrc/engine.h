@@ -101,6 +101,7 @@ struct Pass {
   uint32_t gates;      // gates consumed (stats / cost model)
   // cost-model features: non-diagonal ops on lane qubits, all non-diagonal ops, diagonal ops
   uint32_t lane_ops = 0, dense_ops = 0, diag_ops = 0;
+  uint32_t fma_per_amp = 0;  // tile pass: real multiply-adds per amplitude
 };
 
 // ---------------------------------------------------------------------------

@@ -496,6 +496,13 @@ uint32_t append_op(Plan* P, const Lowered& L, Op op) {
 // Cost-model features of a pass from the ops it applies.
 void count_ops(const std::vector<const Lowered*>& ops, Pass* ps) {
   for (const Lowered* L : ops) {
+    switch (L->op.type) {  // a complex multiply-add is 4 real ones
+      case OP_1Q: ps->fma_per_amp += 8; break;
+      case OP_2Q: ps->fma_per_amp += 16; break;
+      case OP_KQ: ps->fma_per_amp += 4u << L->op.nq; break;
+      case OP_CPHASE: case OP_DIAG: case OP_POLY: ps->fma_per_amp += 4; break;
+      default: break;  // X and sign flips move or negate
+    }
     if (L->nondiag) {
       ++ps->dense_ops;
       if (L->nondiag & 0x1Full) ++ps->lane_ops;

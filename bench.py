@@ -405,6 +405,12 @@ def learned_choice(be, n, flat, precision):
         model.free()
 
 
+def learned_greedy():
+    from aleph_b200 import learned
+
+    return learned.GREEDY
+
+
 def qaoa_sweep_bench(dev: int, sets: int, loop_sample: int, seed: int, ranks: "Ranks") -> dict:
     """Batched QAOA Max-Cut sweep: `sets` parameter sets, n uniform in 12..24,
     random 3-regular graphs (odd n: random graphs with 3n/2 edges), p = 4,
@@ -747,21 +753,36 @@ def run_engine(args, ranks: Ranks):
                 "kernels": kernel_table(per64, peak)}
         # The plain FP64 passes fuse many gates each, so their roofline is
         # max(bytes / HBM, DFMA / the FP64 rate), with the DFMA rate measured
-        # on this GPU (aleph_b200_fp64_rate). Every Haar one-qubit gate costs
-        # 8 DFMA per amplitude (two complex products per output); the CZs are
-        # sign flips.
+        # on this GPU (aleph_b200_fp64_rate). The DFMA are the plan's own: each
+        # pass record counts its real multiply-adds per amplitude (8 per dense
+        # one-qubit op, 16 per fused 4x4); the CZs are sign flips.
         rate = b64.fp64_rate()  # TFLOP/s, 2 flop per DFMA
         n1q = n * depth
-        dfma = 8.0 * n1q * float(1 << n)
+        dfma = sum(r["fma_per_amp"] for r in per64) * float(1 << n) / max(1, args.fp64_steps)
         dfma_s = dfma * 2.0 / (rate * 1e12)
         passes64 = sum(k["launches"] for k in fp64["kernels"].values()) / max(1, args.fp64_steps)
         hbm_s = passes64 * 2.0 * float(1 << n) * 16.0 / (peak * 1e9)
         fp64["roofline"] = {"bound": "max(hbm, fp64)", "fp64_tflops_measured": round(rate, 2), "dfma": dfma,
+                            "dfma_gate_by_gate": 8.0 * n1q * float(1 << n),
                             "dfma_floor_s": round(dfma_s, 4), "hbm_floor_s": round(hbm_s, 4),
                             "passes": passes64, "frac": round(max(dfma_s, hbm_s) / s64_per, 4),
-                            "what": f"{n1q} Haar gates x 8 DFMA x 2^{n} amplitudes at the measured DFMA rate; "
-                                    f"passes x 2 x 2^{n} x 16 B at the measured HBM copy rate"}
+                            "what": f"the plan's multiply-adds per amplitude x 2^{n} at the measured DFMA rate "
+                                    f"({n1q} Haar gates, pair-fused into 4x4s: 16 DFMA per 4x4 where gate by gate "
+                                    f"takes 8 per gate); passes x 2 x 2^{n} x 16 B at the measured HBM copy rate"}
         p64.free()
+        # the same path on the configuration the learned cost model ranks first
+        # (the planner's own choice; the greedy plan above is its baseline)
+        choice64 = learned_choice(b64, n, flat, "f64") if not args.greedy else None
+        if choice64 is not None and choice64 != learned_greedy():
+            choice64.apply(b64)
+            q64 = b64.compile(n, flat)
+            ms_l, per_l, _, _ = time_plan(b64, q64, s64, args.fp64_steps, max(3, args.warmup), ranks, True, None)
+            s_l = ranks.max(ms_l) * 1e-3 / (args.fp64_steps * ranks.world)
+            dfma_l = sum(r["fma_per_amp"] for r in per_l) * float(1 << n) / max(1, args.fp64_steps)
+            fp64["learned"] = {"choice": dict(choice64.__dict__), "s_per_circuit": s_l, "tc32_speedup": s_l / s_per_circuit,
+                               "gain_over_greedy": s64_per / s_l,
+                               "roofline_frac": round(max(dfma_l * 2.0 / (rate * 1e12), hbm_s) / s_l, 4)}
+            q64.free()
         s64.free()
         b64.close()
 

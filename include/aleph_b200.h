@@ -387,7 +387,8 @@ typedef struct aleph_b200_pass_record {
   uint32_t dense_ops;   /* non-diagonal ops the pass applies (a block: the fused gates)    */
   uint32_t diag_ops;    /* diagonal ops the pass applies (phases, CZ-like, DiagonalPhase)  */
   uint32_t variant;     /* kernel variant (tile pass: blocks per SM)                       */
-  uint32_t pad;
+  uint32_t fma_per_amp; /* tile pass: real multiply-adds per amplitude (8 per dense one-qubit
+                           op, 16 per dense 4x4, 4 per diagonal phase; controls ignored)   */
   double ms;            /* device time of the pass (CUDA events on the handle's stream)    */
   double bytes;         /* algorithmic HBM bytes of the pass                               */
 } aleph_b200_pass_record;
