@@ -143,6 +143,75 @@ __device__ __forceinline__ void reg_2q(V2<Real> (&v)[1 << R], const V2<Real>* m,
   }
 }
 
+// The q-th register index with bits JA and JB clear (q's bits deposited in order).
+template <int R, int JA, int JB>
+__device__ constexpr int quartet_base(int q) {
+  int r = 0, bit = 0;
+  for (int j = 0; j < R; ++j) {
+    if (j == JA || j == JB) continue;
+    if ((q >> bit) & 1) r |= 1 << j;
+    ++bit;
+  }
+  return r;
+}
+
+// One row of a 4x4: c0 x0 + c1 x1 + c2 x2 + c3 x3 as one multiply-add chain
+// per component (1 multiply + 7 fused multiply-adds).
+template <typename Real>
+__device__ __forceinline__ V2<Real> mac4(V2<Real> c0, V2<Real> x0, V2<Real> c1, V2<Real> x1, V2<Real> c2, V2<Real> x2,
+                                         V2<Real> c3, V2<Real> x3) {
+  Real re = c0.x * x0.x, im = c0.x * x0.y;
+  re = fma(-c0.y, x0.y, re);
+  im = fma(c0.y, x0.x, im);
+  re = fma(c1.x, x1.x, re);
+  im = fma(c1.x, x1.y, im);
+  re = fma(-c1.y, x1.y, re);
+  im = fma(c1.y, x1.x, im);
+  re = fma(c2.x, x2.x, re);
+  im = fma(c2.x, x2.y, im);
+  re = fma(-c2.y, x2.y, re);
+  im = fma(c2.y, x2.x, im);
+  re = fma(c3.x, x3.x, re);
+  im = fma(c3.x, x3.y, im);
+  re = fma(-c3.y, x3.y, re);
+  im = fma(c3.y, x3.x, im);
+  return mk<Real>(re, im);
+}
+
+// Uncontrolled 4x4 on register bits JA (matrix MSB) > JB, QB quartets at a
+// time: each row of coefficients is loaded once per QB quartets and the
+// block's outputs wait in registers until its inputs are spent. The
+// coefficients are uniform across the warp, and with the tile in registers
+// they cannot all stay live; loaded per quartet, they were most of the pass's
+// L1 traffic.
+template <typename Real, int R, int JA, int JB, int QB>
+__device__ __forceinline__ void reg_2q_blocked(V2<Real> (&v)[1 << R], const V2<Real>* m) {
+  constexpr int NQ = 1 << (R - 2);
+  constexpr int A = 1 << JA, B = 1 << JB;
+#pragma unroll
+  for (int q0 = 0; q0 < NQ; q0 += QB) {
+    V2<Real> o[QB][4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const V2<Real> c0 = ld_coef<Real>(m + 4 * k), c1 = ld_coef<Real>(m + 4 * k + 1),
+                     c2 = ld_coef<Real>(m + 4 * k + 2), c3 = ld_coef<Real>(m + 4 * k + 3);
+#pragma unroll
+      for (int j = 0; j < QB; ++j) {
+        const int r = quartet_base<R, JA, JB>(q0 + j);
+        o[j][k] = mac4<Real>(c0, v[r], c1, v[r | B], c2, v[r | A], c3, v[r | A | B]);
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < QB; ++j) {
+      const int r = quartet_base<R, JA, JB>(q0 + j);
+      v[r] = o[j][0];
+      v[r | B] = o[j][1];
+      v[r | A] = o[j][2];
+      v[r | A | B] = o[j][3];
+    }
+  }
+}
+
 // ---- lane-qubit ops (qubits 0..4, warp shuffles) ----------------------------
 template <typename Real, int R>
 __device__ __forceinline__ void lane_1q(V2<Real> (&v)[1 << R], int s, const V2<Real>* m, bool thr, uint32_t creg) {
@@ -302,9 +371,11 @@ __device__ __forceinline__ void dispatch_pair(int j1, int j2, V2<Real> (&v)[1 <<
 #undef AB_PR
 }
 
-template <typename Real, int R>
+template <typename Real, int R, int QB>
 __device__ __forceinline__ void dispatch_2q(const Op& op, V2<Real> (&v)[1 << R], const V2<Real>* m, bool thr) {
   const uint32_t creg = op.creg;
+  // quartets per coefficient load in the uncontrolled register-register case
+  constexpr int kQB = QB > (1 << (R >= 2 ? R - 2 : 0)) ? (1 << (R >= 2 ? R - 2 : 0)) : QB;
   if (op.b < 5) {
     if (op.a < 5) {
       lane_2q<Real, R>(v, op.a, op.b, m, thr, creg);
@@ -319,9 +390,12 @@ __device__ __forceinline__ void dispatch_2q(const Op& op, V2<Real> (&v)[1 << R],
     }
     return;
   }
-#define AB_RR(a, b)                                    \
-  case (a)*8 + (b):                                    \
-    if constexpr (R > (a)) reg_2q<Real, R, (a), (b)>(v, m, thr, creg); \
+#define AB_RR(a, b)                                                           \
+  case (a)*8 + (b):                                                           \
+    if constexpr (R > (a)) {                                                  \
+      if (kQB > 1 && thr && creg == 0) reg_2q_blocked<Real, R, (a), (b), kQB>(v, m); \
+      else reg_2q<Real, R, (a), (b)>(v, m, thr, creg);                        \
+    }                                                                         \
     break;
   switch ((op.a - 5) * 8 + (op.b - 5)) {
     AB_RR(1, 0) AB_RR(2, 0) AB_RR(2, 1) AB_RR(3, 0) AB_RR(3, 1)
@@ -339,6 +413,15 @@ __global__ void __launch_bounds__(128, OCC) tile_kernel(V2<Real>* __restrict__ a
                                                         const Op* __restrict__ ops, const V2<Real>* __restrict__ coef,
                                                         const PolyTables poly) {
   constexpr int NR = 1 << R;
+  // quartets of a 4x4 per coefficient load: what the register budget
+  // (65536 / (128 * OCC), at most 255) leaves beside the tile's amplitudes
+  // for QB x 4 outputs and a row of coefficients
+  constexpr int kRegBudget = 65536 / (128 * OCC) > 255 ? 255 : 65536 / (128 * OCC);
+  constexpr int kRegData = (1 << R) * 2 * (int)sizeof(Real) / 4;
+  constexpr int kCplx = 2 * (int)sizeof(Real) / 4;  // registers per complex value
+  constexpr int kQuartetBlock = kRegBudget - kRegData >= (16 + 4) * kCplx + 56   ? 4
+                                : kRegBudget - kRegData >= (8 + 4) * kCplx + 56 ? 2
+                                                                                 : 1;
   const int lane = threadIdx.x & 31;
   const uint64_t warp = (uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (warp >= (1ull << (p.n - 5 - R))) return;
@@ -396,7 +479,7 @@ __global__ void __launch_bounds__(128, OCC) tile_kernel(V2<Real>* __restrict__ a
         else dispatch_reg<Real, R>(op, v, m, thr);
         break;
       case OP_2Q:
-        dispatch_2q<Real, R>(op, v, m, thr);
+        dispatch_2q<Real, R, kQuartetBlock>(op, v, m, thr);
         break;
       default:
         diag_ops<Real, R>(op, v, gl, hb, coef, poly);
