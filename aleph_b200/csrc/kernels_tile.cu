@@ -419,7 +419,7 @@ __global__ void __launch_bounds__(128, OCC) tile_kernel(V2<Real>* __restrict__ a
   constexpr int kRegBudget = 65536 / (128 * OCC) > 255 ? 255 : 65536 / (128 * OCC);
   constexpr int kRegData = (1 << R) * 2 * (int)sizeof(Real) / 4;
   constexpr int kCplx = 2 * (int)sizeof(Real) / 4;  // registers per complex value
-  constexpr int kQuartetBlock = kRegBudget - kRegData >= (16 + 4) * kCplx + 56   ? 4
+  constexpr int kQuartetBlock = kRegBudget - kRegData >= (16 + 4) * kCplx + 40   ? 4
                                 : kRegBudget - kRegData >= (8 + 4) * kCplx + 56 ? 2
                                                                                  : 1;
   const int lane = threadIdx.x & 31;
