@@ -140,7 +140,10 @@ __device__ __forceinline__ void rx_regs(V2<Real> (&v)[NR], uint32_t mask, Real c
 // take the same form x' = c x - i s y.
 template <typename Real, int NR>
 __device__ __forceinline__ void rx_lanes(V2<Real> (&v)[NR], uint32_t mask, Real c, Real s) {
-#pragma unroll
+  // FP32: the lane bit is a runtime shuffle mask, so a rolled loop keeps one
+  // copy of the body (unrolled, the FP32 sweeps stall on instruction fetch;
+  // rolled they ran 4% faster). FP64 keeps it unrolled (2% faster so).
+#pragma unroll(sizeof(Real) == 4 ? 1 : 5)
   for (int k = 0; k < 5; ++k) {
     if (!((mask >> k) & 1u)) continue;
 #pragma unroll
