@@ -323,3 +323,28 @@ def test_paged_segments_errors():
         describe_paged(10, c.instructions, 10, 12)
     with pytest.raises(B.InvalidArgument):
         describe_paged(10, c.instructions, 4, 3)
+
+
+def test_pair_fusion_keeps_every_gate_and_never_adds_arithmetic():
+    """Pair fusion (planner.cpp fuse_pairs), host only: every gate lands in
+    exactly one pass, and the plan's real multiply-adds per amplitude never
+    grow (a block is fused only when its gates cost at least 24 per amplitude,
+    against 16 for the 4x4)."""
+    from aleph_b200.backend import describe_plan
+    from tests.circuit_gen import random_circuit
+
+    circuits = [(n, random_circuit(n, 300, seed=s)) for n, s in ((14, 1), (17, 2), (20, 3))]
+    circuits += [(n, workloads.brickwall(n, 12, seed=n)) for n in (14, 22, 31)]
+    circuits += [(24, workloads.qft_product(24, seed=4))]
+    for n, c in circuits:
+        for prec in ("f64", "f32"):
+            for r in (2, 4, 5):
+                on = describe_plan(n, c.instructions, prec, tile_r=r, smem_max_n=0)
+                off = describe_plan(n, c.instructions, prec, tile_r=r, smem_max_n=0, pair_fusion=False)
+                assert sum(p["gates"] for p in on) == sum(p["gates"] for p in off) == c.gate_count()
+                assert sum(p["fma_per_amp"] for p in on) <= sum(p["fma_per_amp"] for p in off)
+    # the brickwall's even-layer blocks halve its arithmetic
+    c = workloads.brickwall(32, 40, seed=0)
+    on = describe_plan(32, c.instructions, "f64")
+    off = describe_plan(32, c.instructions, "f64", pair_fusion=False)
+    assert 2 * sum(p["fma_per_amp"] for p in on) == sum(p["fma_per_amp"] for p in off)
